@@ -1,0 +1,342 @@
+"""Benchmark: node-replica-steps/s of the Monte Carlo SEIR replay on B200.
+
+One bench step = one full replay of the replica-sweep workload (N=100,000
+nodes in 100 communities, 20M contacts over 14 days, 336 one-hour steps,
+4,096 replicas = 64 beta values x 64 seeds, 20 initial infected) through the
+batched bit-packed path with the window CSR built inside the step loop.
+Extra keys report the same replay with prebuilt window CSRs and through the
+plain per-replica SpMV path, the dominant kernel's HBM roofline, and the
+C oracle's CPU throughput on a bounded sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With torchrun (N > 1) every rank replays its own replicas (different seed):
+replicas shard with no data-path collective ("scaling": "weak").
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-replica-steps/s"
+UNIT = "node-replica-steps/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["sweep", "small"], default="sweep")
+    ap.add_argument("--no-extras", action="store_true", help="skip plain-path / CPU / e2e legs")
+    return ap.parse_args()
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def workload(name):
+    from replay_b200 import synthetic
+    return synthetic.replica_sweep() if name == "sweep" else synthetic.small_seir()
+
+
+def algorithmic_bytes(n, m, steps, nnz_total):
+    """Lower-bound HBM bytes of the batched step kernel over one replay:
+    per step 4(N+1) CSR row pointers + 8 n_z CSR pairs + 4 W n_z gathered
+    mask words + 4 W N mask writes + 2 (2/8) N M state planes read+written +
+    16 M count bytes, W = ceil(M/32)."""
+    w = (m + 31) // 32
+    return steps * (4 * (n + 1) + 4 * w * n + 0.5 * n * m + 16 * m) + (8 + 4 * w) * nnz_total
+
+
+def plain_bytes(n, m, steps, nnz_total):
+    """Per-replica SpMV path, same metric: each replica re-reads the CSR and
+    gathers 4 B per entry, writes 4 B exposure per node, plus state r/w."""
+    return m * (steps * (4 * (n + 1) + 4 * n) + 12 * nnz_total) + steps * 0.5 * n * m
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import replay_b200
+
+    torch.cuda.set_device(local_rank)
+    dev = local_rank
+    net = workload(args.workload)
+    p = dict(net["params"])
+    p["seed"] = 1 + rank
+    n_nodes = net["n_nodes"]
+    M, T = p["M"], p["iterations"]
+    nrs_per_replay = n_nodes * M * T
+
+    t0 = time.perf_counter()
+    g = replay_b200.Graph.from_arrays(net["start"], net["end"], net["u"], net["v"], n_nodes, device=dev)
+    ingest_s = time.perf_counter() - t0
+    sim = replay_b200.Simulation(g, path="batched", csr="per-step", **p)
+    sim_pre = replay_b200.Simulation(g, path="batched", csr="prebuilt", **p)
+    info = sim.info
+    info_pre = sim_pre.info
+
+    stream = torch.cuda.Stream(device=dev)
+
+    def timed(s, k, w):
+        with torch.cuda.stream(stream):
+            for _ in range(w):
+                s.enqueue(stream.cuda_stream)
+            torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(k):
+                s.enqueue(stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device=f"cuda:{dev}")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    with ClockSampler(dev) as clk:
+        ms_total = timed(sim, args.steps, args.warmup)
+    clocks = clk.summary()
+    ms_step = ms_total / args.steps
+    value = nrs_per_replay * world / (ms_step / 1e3)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u32 replica bit planes, int32/int64 exact contact-second sums",
+           "data": "synthetic (seeded generator with the workload's shapes and distributions)",
+           "config": {"workload": net["name"], "nodes": n_nodes, "contacts": int(len(net["start"])),
+                      "replicas": M, "steps": T, "path": "batched bit-packed SpMM, window CSR built per step",
+                      "parallelism": f"replicas x{world} (independent ranks)",
+                      "l2": "state planes + CSRs exceed L2 (126 MB); no flush"},
+           "clocks": clocks,
+           "gpu_launches": info["kernels_per_run"] * args.steps}
+
+    # ---- prebuilt-CSR variant ----
+    ms_pre = timed(sim_pre, args.steps, 1) / args.steps
+    out["prebuilt_csr"] = {"value": nrs_per_replay * world / (ms_pre / 1e3), "ms_per_step": ms_pre,
+                           "prebuilt_nnz": info_pre["prebuilt_nnz"]}
+
+    # ---- roofline of the dominant kernel (k_packed_step) ----
+    hbm, peak_kind = load_peaks()
+    prof = sim_pre.profile()
+    nnz_total = info_pre["nnz_total"]
+    bytes_replay = algorithmic_bytes(n_nodes, M, T, nnz_total)
+    step_launch_ms = prof["step_ms"] / max(1, prof["step_launches"])
+    achieved = (bytes_replay / T) / (step_launch_ms / 1e3) / 1e9
+    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                       "frac": achieved / hbm, "peak_source": peak_kind,
+                       "kernel": "k_packed_step", "algorithmic_bytes_per_launch": bytes_replay / T,
+                       "avg_launch_us": step_launch_ms * 1e3, "traffic": None}
+    prof_ps = sim.profile()
+    out["profile_ms"] = {"prebuilt": prof, "per_step": prof_ps}
+
+    if not args.no_extras and rank == 0:
+        # ---- plain per-replica SpMV path (drop-in), same workload ----
+        sim_plain = replay_b200.Simulation(g, path="plain", csr="prebuilt", **p)
+        ms_plain = timed(sim_plain, 1, 1)
+        plain_value = nrs_per_replay / (ms_plain / 1e3)
+        out["plain_path"] = {"value": plain_value, "ms_per_step": ms_plain,
+                             "batched_over_plain": (nrs_per_replay / (ms_pre / 1e3)) / plain_value,
+                             "algorithmic_bytes": plain_bytes(n_nodes, M, T, nnz_total)}
+        del sim_plain
+        # ---- end to end through the public API with host buffers ----
+        e2e_steps = 2
+        h2d = sum(int(net[k].nbytes) for k in ("start", "end", "u", "v")) + 4 * M
+        d2h = (T + 1) * M * 4 * 4
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ge = replay_b200.Graph.from_arrays(net["start"], net["end"], net["u"], net["v"], n_nodes, device=dev)
+            se = replay_b200.Simulation(ge, path="batched", csr="per-step", **p)
+            counts = se.run()
+            se.close()
+            ge.close()
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        out["e2e"] = {"value": nrs_per_replay / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                      "d2h_bytes_per_step": d2h, "s_per_step": e2e_s,
+                      "includes": "contact upload + interval index build + plan + replay + counts readback"}
+        out["ingest_s"] = ingest_s
+        assert counts.shape == (T + 1, M, 4)
+        # ---- CPU baseline: the C oracle on a bounded sample ----
+        out["cpu_baseline"] = cpu_baseline(net, p)
+    return out
+
+
+def cpu_baseline(net, p, m_sample=32, t_sample=24):
+    """The oracle (single-threaded C restatement) on the same network with a
+    reduced replica count and step count; loop time = t(T) - t(0)."""
+    from oracle import orc
+    kw = dict(n_replicas=m_sample, step_size=p["step_size"], window=p["window"], start_time=p["start_time"],
+              transition=1, seed=1, beta=float(np.median(p.get("beta_per_replica", [p.get("beta", 2e-5)]))),
+              p_ei=p.get("p_ei", 0.0), p_ir=p.get("p_ir", 0.0), initial_count=p.get("initial_count", 10),
+              has_exposed=int(p.get("has_exposed", True)))
+    t0 = time.perf_counter()
+    orc.run(net["start"], net["end"], net["u"], net["v"], net["n_nodes"], n_steps=0, **kw)
+    t1 = time.perf_counter()
+    orc.run(net["start"], net["end"], net["u"], net["v"], net["n_nodes"], n_steps=t_sample, **kw)
+    t2 = time.perf_counter()
+    loop = (t2 - t1) - (t1 - t0)
+    return {"value": net["n_nodes"] * m_sample * t_sample / loop, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"same network, {m_sample} replicas x {t_sample} steps; loop time = t({t_sample} steps) - t(0)"}
+
+
+# ---------------------------------------------------------------------------
+def reference_sample(workload_name):
+    """A bounded sample of the workload for the reference CPU path: the first
+    5 communities (5,000 nodes) with the contacts among them, 64 replicas,
+    all 336 steps, countdown durations equal to the geometric means."""
+    net = workload(workload_name)
+    if workload_name == "sweep":
+        keep_n = 5000
+        sel = (net["u"] < keep_n) & (net["v"] < keep_n)
+        sample = {k: net[k][sel] for k in ("start", "end", "u", "v")}
+        sample["n_nodes"] = keep_n
+        m = 64
+    else:
+        sample = {k: net[k] for k in ("start", "end", "u", "v")}
+        sample["n_nodes"] = net["n_nodes"]
+        m = 100
+    return net, sample, m
+
+
+def run_reference(args):
+    from oracle import ref
+    from replay_b200 import synthetic
+    net, sample, m = reference_sample(args.workload)
+    p = net["params"]
+    T = p["iterations"]
+    if not os.path.exists(ref.REPLAY_REF):
+        return {"impl": "reference", "unavailable": "oracle/_ref/replay_ref was not built (reference tree absent at build time)"}
+    beta = float(np.median(p.get("beta_per_replica", [p.get("beta", 2e-5)])))
+    infect_prob = 1.0 - np.exp(-beta * 3600.0)
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "contacts.txt")
+        synthetic.write_contact_file(path, sample)
+        base = [path, "--cpu-only", "--cpu-threads", cores, "-q", "--M", m, "--step-size", p["step_size"],
+                "--static-network-duration", p["window"], "--start-time", p["start_time"],
+                "--initial-infected", p["initial_count"] / sample["n_nodes"], "--infect-prob", infect_prob,
+                "--exposed-duration", int(3600 / max(p.get("p_ei", 1 / 48), 1e-9)),
+                "--infectious-duration", int(3600 / p["p_ir"]), "--resistant-duration", 10 ** 8]
+        times = []
+        for it in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            r0 = ref.run_cli(base + ["--iterations", 0])
+            t1 = time.perf_counter()
+            r1 = ref.run_cli(base + ["--iterations", T])
+            t2 = time.perf_counter()
+            if r0.returncode or r1.returncode:
+                return {"impl": "reference", "unavailable": f"reference exited {r0.returncode}/{r1.returncode}"}
+            if it >= args.warmup:
+                times.append((t2 - t1) - (t1 - t0))
+    loop = statistics.median(times)
+    value = sample["n_nodes"] * m * T / loop
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": loop * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32 countdowns, fp32 exposures",
+            "data": "synthetic", "config": {"workload": net["name"], "sample_nodes": sample["n_nodes"],
+                                            "sample_contacts": int(len(sample["start"])), "replicas": m,
+                                            "steps": T},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"first {sample['n_nodes']} nodes' contacts, {m} replicas, {T} steps, "
+                                       "replay --cpu-only, loop = t(iterations=T) - t(iterations=0)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device(f"cuda:{local_rank}"))
+    out = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,201 @@
+"""replay_b200: Monte Carlo SEIR replay over temporal contact networks on B200.
+
+Python mirror of the `replay` command line (the reference's only interface,
+tool/gpu_cpu_temporal_sim.cu:570-699) over the libreplay C ABI:
+
+    g = Graph.load("contacts.txt")              # NODE_LIST + `u, v, t0, t1;` lines
+    sim = Simulation(g, M=1000, iterations=168, step_size=3600,
+                     initial_infected=0.01, infect_prob=0.0695,
+                     exposed_duration=172800, infectious_duration=432000)
+    counts = sim.run()                           # (iterations+1, M, 4) int32
+    # columns: exposed, infectious, resistant, susceptible (summary CSV order)
+
+Keyword names follow the CLI flags (--M, --iterations, --step-size,
+--initial-infected, --infect-prob, --exposed-duration, ...); the additive
+geometric mode takes transition="geometric", beta, p_ei, p_ir, p_rs.
+Every simulation runs on the GPU; there is no CPU fallback.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import CLI_PATH, ReplayError, check, lib
+
+__all__ = ["Graph", "Simulation", "ReplayError", "window_csr", "CLI_PATH", "version"]
+
+
+def version():
+    return lib().rp_version().decode()
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class Graph:
+    """A contact network held on one GPU (interval index + contacts)."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def load(cls, path, device=0):
+        h = C.c_void_p()
+        check(lib().rp_graph_load_text(str(path).encode(), device, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_arrays(cls, start, end, u, v, n_nodes, device=0):
+        start = np.ascontiguousarray(start, np.int64)
+        end = np.ascontiguousarray(end, np.int64)
+        u = np.ascontiguousarray(u, np.int32)
+        v = np.ascontiguousarray(v, np.int32)
+        h = C.c_void_p()
+        check(lib().rp_graph_from_arrays(_ptr(start), _ptr(end), _ptr(u), _ptr(v), len(start), int(n_nodes),
+                                         device, C.byref(h)))
+        return cls(h.value)
+
+    @property
+    def info(self):
+        gi = _lib.GraphInfo()
+        check(lib().rp_graph_get_info(self._h, C.byref(gi)))
+        return {k: getattr(gi, k) for k, _ in gi._fields_}
+
+    @property
+    def n_nodes(self):
+        return self.info["n_nodes"]
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().rp_graph_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def window_csr(graph, ws, we, scale=1.0, weight="f32", ncls_cap=True):
+    """Canonical symmetric CSR of window [ws, we) built on the GPU.
+
+    weight "f32": (float)overlap*scale merged in hit order (the reference's
+    build_csr_from_intervals); "i32": integer contact-seconds.
+    Returns (row_ptr, col, val, n_hits)."""
+    n = graph.n_nodes
+    kind = 0 if weight == "f32" else 1
+    row_ptr = np.zeros(n + 1, np.int32)
+    nnz, nh = C.c_int64(), C.c_int64()
+    cap = 1
+    while True:
+        col = np.zeros(cap, np.int32)
+        val = np.zeros(cap, np.float32 if kind == 0 else np.int32)
+        st = lib().rp_window_csr(graph._h, int(ws), int(we), float(scale), kind, 1 if ncls_cap else 0,
+                                 _ptr(row_ptr), _ptr(col), _ptr(val), cap, C.byref(nnz), C.byref(nh))
+        if st == 6 and nnz.value > cap:  # RP_ERR_RANGE: grow to the reported size
+            cap = nnz.value
+            continue
+        check(st)
+        return row_ptr, col[: nnz.value], val[: nnz.value], nh.value
+
+
+class Simulation:
+    """One replay configuration on a Graph (device state owned here).
+
+    Keyword arguments mirror rp_params / the CLI flags:
+      M (n_replicas), iterations (n_steps), step_size, start_time, window
+      (static network duration), transition ("countdown" | "geometric"),
+      path ("auto" | "plain" | "batched"), csr ("per-step" | "prebuilt"),
+      seed, exposed_duration, infectious_duration, resistant_duration,
+      infect_prob, initial_infected, initial_count, beta, beta_per_replica,
+      susceptibility, p_ei, p_ir, p_rs, has_exposed, ir_to_s, ncls_cap,
+      record_node_states.
+    """
+
+    _ALIASES = {"M": "n_replicas", "iterations": "n_steps", "static_network_duration": "window",
+                "time_step": "window"}
+
+    def __init__(self, graph, **kw):
+        self.graph = graph
+        p = _lib.Params()
+        lib().rp_params_default(C.byref(p))
+        self._keep = []
+        for k, val in kw.items():
+            k = self._ALIASES.get(k, k)
+            if k == "transition":
+                val = _lib.TRANSITION[val] if isinstance(val, str) else int(val)
+            elif k == "path":
+                val = _lib.PATH[val] if isinstance(val, str) else int(val)
+            elif k == "csr":
+                k, val = "csr_mode", (_lib.CSR_MODE[val] if isinstance(val, str) else int(val))
+            elif k in ("beta_per_replica", "susceptibility"):
+                if val is None:
+                    continue
+                arr = np.ascontiguousarray(val, np.float32)
+                self._keep.append(arr)
+                val = arr.ctypes.data
+            elif k in ("ncls_cap", "has_exposed", "ir_to_s", "record_node_states"):
+                val = int(bool(val))
+            if not hasattr(p, k) or k == "struct_size":
+                raise TypeError(f"unknown simulation parameter {k!r}")
+            setattr(p, k, val)
+        self.params = p
+        h = C.c_void_p()
+        check(lib().rp_sim_create(graph._h, C.byref(p), C.byref(h)))
+        self._h = h
+        self.M, self.T = p.n_replicas, p.n_steps
+
+    @property
+    def info(self):
+        si = _lib.SimInfo()
+        check(lib().rp_sim_get_info(self._h, C.byref(si)))
+        return {k: getattr(si, k) for k, _ in si._fields_}
+
+    def run(self, node_states=None):
+        """Runs the replay; returns counts (T+1, M, 4) as (E, I, R, S).
+
+        node_states: optional callable(step_index, timestamp, states[M, N])
+        (requires record_node_states=True)."""
+        counts = np.zeros((self.T + 1) * self.M * 4, np.int32)
+        if node_states is not None:
+            def _cb(user, step_index, ts, states, n, m):
+                arr = np.ctypeslib.as_array(states, shape=(m * n,)).reshape(m, n).copy()
+                return int(bool(node_states(step_index, ts, arr)))
+            cb = _lib.STATE_CB(_cb)
+        else:
+            cb = _lib.STATE_CB()
+        check(lib().rp_sim_run(self._h, _ptr(counts), cb, None))
+        return counts.reshape(self.T + 1, self.M, 4)
+
+    def profile(self):
+        """Device time per kernel group of one eager replay (CUDA events)."""
+        pr = _lib.Profile()
+        check(lib().rp_sim_profile(self._h, C.byref(pr)))
+        return {k: getattr(pr, k) for k, _ in pr._fields_}
+
+    def enqueue(self, stream=None):
+        """Enqueues the whole replay on a CUDA stream handle (int) without sync."""
+        check(lib().rp_sim_enqueue(self._h, C.c_void_p(stream) if stream else None))
+
+    def counts(self):
+        counts = np.zeros((self.T + 1) * self.M * 4, np.int32)
+        check(lib().rp_sim_counts(self._h, _ptr(counts)))
+        return counts.reshape(self.T + 1, self.M, 4)
+
+    def timestamps(self):
+        ts = np.zeros(self.T + 1, np.int64)
+        check(lib().rp_sim_timestamps(self._h, _ptr(ts)))
+        return ts
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().rp_sim_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,634 @@
+// Contact-file ingest and the device interval index.
+//
+// Replaces tool/temporal_contact_matrix.c (parse_edgelist_build_intervals
+// :148-321, count_valid_edges :122-143, parse_iso8601_to_unix :95-120,
+// get_or_create_node_index :328-356) and the NCLS build
+// (tool/ncls/ncls/src/intervaldb.c:227-326).
+//
+// The file format and its acceptance rules are the reference's:
+//  * line 1 starts with "NODE_LIST" + blank; its tokens are non-negative
+//    base-10 ids without duplicates; N = token count;
+//  * the contact lines a line-counting pass accepts with the pattern
+//    " %d, %d, %63[^,], %63[^;];" bound the number of contacts; the parse
+//    pass reads " %d , %d , %63[^,] , %63[^;\r\n] ;" and skips (and counts
+//    as malformed) lines it cannot read; lines starting with '#' are
+//    comments; lines are read in fgets chunks of at most 99,999 chars;
+//  * timestamps are "%d-%d-%dT%d:%d:%d" in UTC with timegm's normalisation
+//    of out-of-range fields; a timestamp equal to -1 rejects the line;
+//  * node index = order of first appearance in contact lines.
+// Canonical lines take a hand-written fast path (parallel over threads);
+// every other line goes through sscanf with the reference's two patterns.
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
+#include <climits>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+
+#include "rp_internal.h"
+
+namespace rp {
+namespace {
+
+constexpr size_t kFgetsChunk = 99999;  // fgets(buf, 100000, fp)
+
+int64_t floor_div64(int64_t a, int64_t b) {
+  int64_t q = a / b;
+  if ((a % b != 0) && ((a < 0) != (b < 0))) --q;
+  return q;
+}
+
+// Proleptic Gregorian day number of y-m-d relative to 1970-01-01
+// (H. Hinnant's days_from_civil).
+int64_t days_from_civil(int64_t y, int64_t m, int64_t d) {
+  y -= m <= 2;
+  const int64_t era = (y >= 0 ? y : y - 399) / 400;
+  const int64_t yoe = y - era * 400;
+  const int64_t doy = (153 * (m > 2 ? m - 3 : m + 9) + 2) / 5 + d - 1;
+  const int64_t doe = yoe * 365 + yoe / 4 - yoe / 100 + doy;
+  return era * 146097 + doe - 719468;
+}
+
+int64_t utc_seconds(int64_t year, int64_t month, int64_t day, int64_t hour,
+                    int64_t minute, int64_t second) {
+  const int64_t m0 = month - 1;
+  const int64_t y = year + floor_div64(m0, 12);
+  const int64_t m = m0 - floor_div64(m0, 12) * 12;
+  return (days_from_civil(y, m + 1, 1) + day - 1) * 86400 + hour * 3600 +
+         minute * 60 + second;
+}
+
+int64_t iso8601_slow(const char *s) {
+  int year, month, day, hour, min, sec;
+  char extra[10];
+  if (sscanf(s, "%d-%d-%dT%d:%d:%d%9s", &year, &month, &day, &hour, &min, &sec,
+             extra) < 6)
+    return -1;
+  return utc_seconds(year, month, day, hour, min, sec);
+}
+
+struct Contact {
+  int64_t s, e;
+  int32_t a, b;  // raw ids
+};
+
+struct ChunkResult {
+  std::vector<Contact> contacts;
+  int64_t counted = 0;
+  int64_t malformed = 0;
+};
+
+inline bool is_blank(char c) { return c == ' ' || c == '\t'; }
+inline bool is_digit(char c) { return c >= '0' && c <= '9'; }
+
+// Parses [-]digits (1..9 digits) at p.
+inline bool fast_int(const char *&p, const char *end, int64_t &out) {
+  bool neg = false;
+  if (p < end && *p == '-') {
+    neg = true;
+    ++p;
+  }
+  int n = 0;
+  int64_t v = 0;
+  while (p < end && is_digit(*p) && n < 10) {
+    v = v * 10 + (*p - '0');
+    ++p;
+    ++n;
+  }
+  if (n == 0 || n > 9) return false;
+  out = neg ? -v : v;
+  return true;
+}
+
+// digits-digits-digitsTdigits:digits:digits[Z] followed by blanks up to `end`
+inline bool fast_ts(const char *p, const char *end, int64_t &out) {
+  int64_t f[6];
+  const char seps[6] = {'-', '-', 'T', ':', ':', 0};
+  for (int i = 0; i < 6; ++i) {
+    int n = 0;
+    int64_t v = 0;
+    while (p < end && is_digit(*p) && n < 10) {
+      v = v * 10 + (*p - '0');
+      ++p;
+      ++n;
+    }
+    if (n == 0 || n > 9) return false;
+    f[i] = v;
+    if (i < 5) {
+      if (p >= end || *p != seps[i]) return false;
+      ++p;
+    }
+  }
+  if (p < end && *p == 'Z') ++p;
+  while (p < end && is_blank(*p)) ++p;
+  if (p != end) return false;
+  out = utc_seconds(f[0], f[1], f[2], f[3], f[4], f[5]);
+  return true;
+}
+
+// Canonical line: [blanks]id,[blanks]id,[blanks]TS[blanks],[blanks]TS[blanks];...
+// Returns false when the line is not canonical (caller falls back).
+inline bool fast_line(const char *p, const char *end, Contact &c) {
+  while (p < end && is_blank(*p)) ++p;
+  int64_t a, b;
+  if (!fast_int(p, end, a) || p >= end || *p != ',') return false;
+  ++p;
+  while (p < end && is_blank(*p)) ++p;
+  if (!fast_int(p, end, b) || p >= end || *p != ',') return false;
+  ++p;
+  while (p < end && is_blank(*p)) ++p;
+  const char *s0 = p;
+  while (p < end && *p != ',' && *p != '\n' && *p != '\r' && *p != ';') ++p;
+  if (p >= end || *p != ',' || p == s0 || p - s0 > 63) return false;
+  const char *s1 = p;
+  ++p;
+  while (p < end && is_blank(*p)) ++p;
+  const char *e0 = p;
+  while (p < end && *p != ';' && *p != '\n' && *p != '\r' && *p != ',') ++p;
+  if (p >= end || *p != ';' || p == e0 || p - e0 > 63) return false;
+  const char *e1 = p;
+  int64_t ts, te;
+  if (!fast_ts(s0, s1, ts) || !fast_ts(e0, e1, te)) return false;
+  c.s = ts;
+  c.e = te;
+  c.a = (int32_t)a;
+  c.b = (int32_t)b;
+  return true;
+}
+
+// One fgets chunk through the reference's two sscanf patterns.
+void slow_chunk(const char *p, size_t len, ChunkResult &r) {
+  std::string line(p, len);
+  if (!line.empty() && line[0] == '#') return;
+  int d1, d2;
+  char s[64], e[64];
+  if (sscanf(line.c_str(), " %d, %d, %63[^,], %63[^;];", &d1, &d2, s, e) == 4)
+    r.counted++;
+  int a, b;
+  if (sscanf(line.c_str(), " %d , %d , %63[^,] , %63[^;\r\n] ;", &a, &b, s, e) != 4) {
+    r.malformed++;
+    return;
+  }
+  const int64_t ts = iso8601_slow(s), te = iso8601_slow(e);
+  if (ts == -1 || te == -1) return;
+  r.contacts.push_back(Contact{ts, te, a, b});
+}
+
+void parse_range(const char *p, const char *end, ChunkResult &r) {
+  while (p < end) {
+    const char *nl = (const char *)memchr(p, '\n', (size_t)(end - p));
+    const char *le = nl ? nl + 1 : end;  // line including '\n'
+    const size_t len = (size_t)(le - p);
+    if (len <= kFgetsChunk) {
+      if (p[0] != '#') {
+        Contact c;
+        if (fast_line(p, le, c)) {
+          r.counted++;
+          if (c.s != -1 && c.e != -1) r.contacts.push_back(c);
+        } else {
+          slow_chunk(p, len, r);
+        }
+      }
+    } else {
+      for (size_t off = 0; off < len; off += kFgetsChunk)
+        slow_chunk(p + off, std::min(kFgetsChunk, len - off), r);
+    }
+    p = le;
+  }
+}
+
+struct IdMap {
+  std::vector<int32_t> keys, vals;
+  std::vector<uint8_t> used;
+  size_t mask = 0, count = 0;
+  explicit IdMap(size_t expect) {
+    size_t cap = 1024;
+    while (cap < 2 * expect + 2) cap <<= 1;
+    keys.resize(cap);
+    vals.resize(cap);
+    used.assign(cap, 0);
+    mask = cap - 1;
+  }
+  static size_t h(int32_t k) {
+    uint64_t x = (uint32_t)k * 0x9E3779B97F4A7C15ull;
+    return (size_t)(x ^ (x >> 31));
+  }
+  void grow() {
+    IdMap big(keys.size());
+    for (size_t i = 0; i < keys.size(); ++i)
+      if (used[i]) big.put(keys[i], vals[i]);
+    *this = std::move(big);
+  }
+  void put(int32_t k, int32_t v) {
+    size_t i = h(k) & mask;
+    while (used[i]) i = (i + 1) & mask;
+    used[i] = 1;
+    keys[i] = k;
+    vals[i] = v;
+    ++count;
+  }
+  int32_t get(int32_t k) const {
+    size_t i = h(k) & mask;
+    while (used[i]) {
+      if (keys[i] == k) return vals[i];
+      i = (i + 1) & mask;
+    }
+    return -1;
+  }
+  int32_t get_or_add(int32_t k) {
+    int32_t v = get(k);
+    if (v >= 0) return v;
+    if (2 * (count + 1) > keys.size()) grow();
+    v = (int32_t)count;
+    put(k, v);
+    return v;
+  }
+};
+
+// Stable LSD radix sort of (key, value) by key, 16-bit digits.
+void radix_sort_u64(std::vector<uint64_t> &key, std::vector<uint32_t> &val) {
+  const size_t n = key.size();
+  std::vector<uint64_t> k2(n);
+  std::vector<uint32_t> v2(n);
+  std::vector<size_t> cnt(65536);
+  for (int sh = 0; sh < 64; sh += 16) {
+    std::fill(cnt.begin(), cnt.end(), 0);
+    for (size_t i = 0; i < n; ++i) cnt[(key[i] >> sh) & 0xFFFF]++;
+    bool trivial = false;
+    for (size_t b = 0; b < 65536; ++b)
+      if (cnt[b] == n) trivial = true;
+    if (trivial) continue;
+    size_t acc = 0;
+    for (size_t b = 0; b < 65536; ++b) {
+      size_t c = cnt[b];
+      cnt[b] = acc;
+      acc += c;
+    }
+    for (size_t i = 0; i < n; ++i) {
+      size_t pos = cnt[(key[i] >> sh) & 0xFFFF]++;
+      k2[pos] = key[i];
+      v2[pos] = val[i];
+    }
+    key.swap(k2);
+    val.swap(v2);
+  }
+}
+
+int bit_width_u64(uint64_t x) {
+  int b = 0;
+  while (x) {
+    ++b;
+    x >>= 1;
+  }
+  return b;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+rp_status parse_contact_file(const char *path, int32_t &n_nodes,
+                             int32_t &n_index, int64_t &n_malformed,
+                             std::vector<int64_t> &start,
+                             std::vector<int64_t> &end, std::vector<int32_t> &u,
+                             std::vector<int32_t> &v) {
+  int fd = open(path, O_RDONLY);
+  if (fd < 0) {
+    set_error("could not open file '%s'", path);
+    return RP_ERR_IO;
+  }
+  struct stat stt;
+  if (fstat(fd, &stt) != 0) {
+    close(fd);
+    set_error("could not stat '%s'", path);
+    return RP_ERR_IO;
+  }
+  const size_t size = (size_t)stt.st_size;
+  const char *data = nullptr;
+  if (size > 0) {
+    data = (const char *)mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fd, 0);
+    if (data == MAP_FAILED) {
+      close(fd);
+      set_error("could not map '%s'", path);
+      return RP_ERR_IO;
+    }
+  }
+  close(fd);
+  struct Unmap {
+    const char *d;
+    size_t n;
+    ~Unmap() {
+      if (d) munmap((void *)d, n);
+    }
+  } unmap{data, size};
+
+  // ---- header ----
+  if (size == 0) {
+    set_error("unable to read first line from file");
+    return RP_ERR_PARSE;
+  }
+  const char *hl_end = (const char *)memchr(data, '\n', size);
+  const size_t hlen = hl_end ? (size_t)(hl_end - data) + 1 : size;
+  std::string header(data, hlen);
+  if (header.compare(0, 9, "NODE_LIST") != 0 || header.size() < 10 ||
+      (header[9] != ' ' && header[9] != '\t')) {
+    set_error("first line must begin with 'NODE_LIST'");
+    return RP_ERR_PARSE;
+  }
+  std::vector<long> ids;
+  {
+    char *save = nullptr;
+    for (char *tok = strtok_r(&header[9], " \t\r\n", &save); tok;
+         tok = strtok_r(nullptr, " \t\r\n", &save)) {
+      errno = 0;
+      char *endp = nullptr;
+      long id = strtol(tok, &endp, 10);
+      if (errno != 0 || *endp != '\0' || id < 0) {
+        set_error("invalid node ID in NODE_LIST: '%s'", tok);
+        return RP_ERR_PARSE;
+      }
+      ids.push_back((long)(int)id);
+    }
+  }
+  if (ids.empty()) {
+    set_error("no valid node IDs found in NODE_LIST");
+    return RP_ERR_PARSE;
+  }
+  {
+    std::vector<long> sorted = ids;
+    std::sort(sorted.begin(), sorted.end());
+    for (size_t i = 1; i < sorted.size(); ++i)
+      if (sorted[i] == sorted[i - 1]) {
+        set_error("duplicate node ID detected in NODE_LIST: %ld", sorted[i]);
+        return RP_ERR_PARSE;
+      }
+  }
+  if (ids.size() > (size_t)INT32_MAX) {
+    set_error("NODE_LIST too long");
+    return RP_ERR_RANGE;
+  }
+  n_nodes = (int32_t)ids.size();
+
+  // ---- contact lines (the header's own fgets chunks are malformed lines) ----
+  int64_t header_chunks = 0;
+  for (size_t off = 0; off < hlen; off += kFgetsChunk) ++header_chunks;
+  unsigned nthreads = std::thread::hardware_concurrency();
+  if (nthreads == 0) nthreads = 1;
+  if (nthreads > 32) nthreads = 32;
+  const char *body = data + hlen, *body_end = data + size;
+  const size_t body_len = (size_t)(body_end - body);
+  if (body_len < (size_t)1 << 20) nthreads = 1;
+  std::vector<const char *> cuts(nthreads + 1);
+  cuts[0] = body;
+  cuts[nthreads] = body_end;
+  for (unsigned t = 1; t < nthreads; ++t) {
+    const char *p = body + body_len * t / nthreads;
+    if (p < cuts[t - 1]) p = cuts[t - 1];
+    const char *nl = (const char *)memchr(p, '\n', (size_t)(body_end - p));
+    cuts[t] = nl ? nl + 1 : body_end;
+  }
+  std::vector<ChunkResult> parts(nthreads);
+  {
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nthreads; ++t)
+      pool.emplace_back([&, t] { parse_range(cuts[t], cuts[t + 1], parts[t]); });
+    for (auto &th : pool) th.join();
+  }
+  int64_t counted = 0, valid = 0;
+  n_malformed = header_chunks;
+  for (auto &pr : parts) {
+    counted += pr.counted;
+    valid += (int64_t)pr.contacts.size();
+    n_malformed += pr.malformed;
+  }
+  if (counted <= 0) {
+    set_error("no valid edge lines found in %s", path);
+    return RP_ERR_PARSE;
+  }
+  if (valid > counted) {
+    set_error("more edges parsed than expected (%lld > %lld)", (long long)valid,
+              (long long)counted);
+    return RP_ERR_PARSE;
+  }
+  if (valid == 0) {
+    set_error("no intervals read or parse error");
+    return RP_ERR_PARSE;
+  }
+  if (valid > (int64_t)INT32_MAX) {
+    set_error("too many contacts (%lld)", (long long)valid);
+    return RP_ERR_RANGE;
+  }
+
+  // ---- node index: first appearance, sequential over the parts ----
+  IdMap map((size_t)n_nodes);
+  for (auto &pr : parts)
+    for (auto &c : pr.contacts) {
+      map.get_or_add(c.a);
+      map.get_or_add(c.b);
+    }
+  n_index = (int32_t)map.count;
+  if (n_index > n_nodes) {
+    set_error("contact lines name %d distinct nodes but NODE_LIST declares %d",
+              n_index, n_nodes);
+    return RP_ERR_PARSE;
+  }
+  start.resize(valid);
+  end.resize(valid);
+  u.resize(valid);
+  v.resize(valid);
+  {
+    std::vector<int64_t> base(nthreads + 1, 0);
+    for (unsigned t = 0; t < nthreads; ++t)
+      base[t + 1] = base[t] + (int64_t)parts[t].contacts.size();
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nthreads; ++t)
+      pool.emplace_back([&, t] {
+        int64_t k = base[t];
+        for (auto &c : parts[t].contacts) {
+          const int32_t ia = map.get(c.a), ib = map.get(c.b);
+          start[k] = c.s;
+          end[k] = c.e;
+          u[k] = ia < ib ? ia : ib;
+          v[k] = ia < ib ? ib : ia;
+          ++k;
+        }
+      });
+    for (auto &th : pool) th.join();
+  }
+  return RP_OK;
+}
+
+// ---------------------------------------------------------------------------
+rp_status graph_build(Graph &g, std::vector<int64_t> &start,
+                      std::vector<int64_t> &end, std::vector<int32_t> &u,
+                      std::vector<int32_t> &v, int32_t n_nodes) {
+  const int64_t n = (int64_t)start.size();
+  g.n_nodes = n_nodes;
+  g.n_contacts = n;
+  if (n > (int64_t)INT32_MAX) {
+    set_error("too many contacts");
+    return RP_ERR_RANGE;
+  }
+  // Stored coordinates: the reference database keeps intervals with a
+  // negative start mirrored as (-end, -(int)start) (ALL_POSITIVE_ORIENTATION,
+  // intervaldb.c:233-235 and :412-424).
+  for (int64_t i = 0; i < n; ++i) {
+    if (start[i] < 0) {
+      const int64_t s = start[i];
+      start[i] = -end[i];
+      end[i] = -(int64_t)(int32_t)s;
+    }
+  }
+  // Order by (start asc, end desc), ties in file order: the reference's
+  // qsort (imstart_qsort_cmp, intervaldb.c:30-46) is glibc's stable merge sort.
+  std::vector<uint32_t> perm(n);
+  for (int64_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
+  if (n > 0) {
+    int64_t smin = start[0], smax = start[0], emin = end[0], emax = end[0];
+    for (int64_t i = 1; i < n; ++i) {
+      smin = std::min(smin, start[i]);
+      smax = std::max(smax, start[i]);
+      emin = std::min(emin, end[i]);
+      emax = std::max(emax, end[i]);
+    }
+    const uint64_t srange = (uint64_t)smax - (uint64_t)smin;
+    const uint64_t erange = (uint64_t)emax - (uint64_t)emin;
+    const int sb = bit_width_u64(srange), eb = bit_width_u64(erange);
+    std::vector<uint64_t> key(n);
+    if (sb + eb <= 64) {
+      for (int64_t i = 0; i < n; ++i)
+        key[i] = (eb == 64 ? 0 : (((uint64_t)start[i] - (uint64_t)smin) << eb)) |
+                 ((uint64_t)emax - (uint64_t)end[i]);
+      radix_sort_u64(key, perm);
+    } else {
+      for (int64_t i = 0; i < n; ++i) key[i] = (uint64_t)emax - (uint64_t)end[i];
+      radix_sort_u64(key, perm);
+      for (int64_t i = 0; i < n; ++i) key[i] = (uint64_t)start[perm[i]] - (uint64_t)smin;
+      radix_sort_u64(key, perm);
+    }
+    g.t_min = smin;
+    g.t_max = emax;
+  }
+  std::vector<int64_t> ss(n), se(n);
+  std::vector<int32_t> su(n), sv(n);
+  for (int64_t i = 0; i < n; ++i) {
+    ss[i] = start[perm[i]];
+    se[i] = end[perm[i]];
+    su[i] = u[perm[i]];
+    sv[i] = v[perm[i]];
+  }
+  // nlists of the nested containment list (intervaldb.c:243-320): one header
+  // per interval with a child plus one per restart of the parent chain, i.e.
+  // (top-level intervals - 1) + (intervals with a child).  i nests in the
+  // nearest open ancestor containing it; identical intervals do not nest.
+  {
+    std::vector<int64_t> chain;
+    chain.reserve(64);
+    std::vector<uint8_t> has_child(n, 0);
+    int64_t n_top = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      while (!chain.empty()) {
+        const int64_t p = chain.back();
+        const bool outside = se[i] > se[p] || (se[i] == se[p] && ss[i] == ss[p]);
+        if (!outside) break;
+        chain.pop_back();
+      }
+      if (chain.empty())
+        ++n_top;
+      else
+        has_child[chain.back()] = 1;
+      chain.push_back(i);
+    }
+    int64_t parents = 0;
+    for (int64_t i = 0; i < n; ++i) parents += has_child[i];
+    g.nlists = n > 0 ? (n_top - 1) + parents : 0;
+  }
+  // Duration classes, stable: class 0 durations <= 1, class c in (2^(c-1), 2^c].
+  std::vector<uint8_t> cls(n);
+  std::vector<int64_t> cnt(kClasses + 1, 0);
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t d = se[i] - ss[i];
+    int c = 0;
+    if (d > 1) c = bit_width_u64((uint64_t)(d - 1));
+    cls[i] = (uint8_t)c;
+    cnt[c + 1]++;
+  }
+  g.class_off.assign(kClasses + 1, 0);
+  for (int c = 0; c < kClasses; ++c) g.class_off[c + 1] = g.class_off[c] + cnt[c + 1];
+  g.n_classes_used = 0;
+  for (int c = 0; c < kClasses; ++c) g.n_classes_used += cnt[c + 1] > 0;
+  std::vector<int64_t> pos(g.class_off.begin(), g.class_off.end() - 1);
+  std::vector<int64_t> cs(n), ce(n);
+  std::vector<int32_t> cu(n), cv(n), cr(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t p = pos[cls[i]]++;
+    cs[p] = ss[i];
+    ce[p] = se[i];
+    cu[p] = su[i];
+    cv[p] = sv[i];
+    cr[p] = (int32_t)i;
+  }
+  g.h_cs = cs;
+  RP_TRY_CUDA(cudaSetDevice(g.device));
+  RP_TRY(g.cs.alloc(sizeof(int64_t) * n));
+  RP_TRY(g.ce.alloc(sizeof(int64_t) * n));
+  RP_TRY(g.cu.alloc(sizeof(int32_t) * n));
+  RP_TRY(g.cv.alloc(sizeof(int32_t) * n));
+  RP_TRY(g.crank.alloc(sizeof(int32_t) * n));
+  if (n > 0) {
+    RP_TRY_CUDA(cudaMemcpy(g.cs.ptr, cs.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
+    RP_TRY_CUDA(cudaMemcpy(g.ce.ptr, ce.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
+    RP_TRY_CUDA(cudaMemcpy(g.cu.ptr, cu.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    RP_TRY_CUDA(cudaMemcpy(g.cv.ptr, cv.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    RP_TRY_CUDA(cudaMemcpy(g.crank.ptr, cr.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  }
+  return RP_OK;
+}
+
+// ---------------------------------------------------------------------------
+static int64_t sat_sub(int64_t a, int64_t b) {  // a - b, b >= 0, saturating
+  if (a < INT64_MIN + b) return INT64_MIN;
+  return a - b;
+}
+
+void plan_window(const Graph &g, int64_t ws, int64_t we, float scale,
+                 int64_t cap, std::vector<CandRange> &ranges, WinDesc &out) {
+  out.ws = ws;
+  out.we = we;
+  out.scale = scale;
+  // The reference mirrors a query whose start is negative (intervaldb.c:437-444).
+  if (ws < 0) {
+    out.qs = -we;
+    out.qe = -ws;
+  } else {
+    out.qs = ws;
+    out.qe = we;
+  }
+  out.range_off = (int32_t)ranges.size();
+  out.n_ranges = 0;
+  out.n_candidates = 0;
+  for (int c = 0; c < kClasses; ++c) {
+    const int64_t b0 = g.class_off[c], b1 = g.class_off[c + 1];
+    if (b1 <= b0) continue;
+    // candidates: stored start in (qs - 2^c, qe)
+    const int64_t span = c >= 63 ? INT64_MAX : ((int64_t)1 << c);
+    const int64_t lo_key = sat_sub(out.qs, span);  // start > lo_key
+    auto first = g.h_cs.begin() + b0, last = g.h_cs.begin() + b1;
+    auto lo = std::upper_bound(first, last, lo_key);
+    auto hi = std::lower_bound(lo, last, out.qe);
+    const int64_t count = hi - lo;
+    if (count <= 0) continue;
+    ranges.push_back(CandRange{(int64_t)(lo - g.h_cs.begin()), count, out.n_candidates});
+    out.n_candidates += count;
+    out.n_ranges++;
+  }
+  out.may_truncate = out.n_candidates > cap ? 1 : 0;
+}
+
+}  // namespace rp

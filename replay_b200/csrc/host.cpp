@@ -1,0 +1,821 @@
+// libreplay host driver: the C ABI of include/replay.h.
+//
+// Replaces the reference driver (tool/gpu_cpu_temporal_sim.cu:570-1185):
+// schedule arithmetic, per-step window queries, CSR construction, the
+// exposure product, transitions and count output -- with all per-step work
+// enqueued on the device and captured once into a CUDA graph, so one replay
+// is one graph launch.  No host synchronisation inside the step loop; only
+// the (n_steps+1) x M x 4 counts leave the device.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "rp_internal.h"
+
+namespace rp {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+rp_status cuda_fail(cudaError_t e, const char *what) {
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  (void)cudaGetLastError();
+  return RP_ERR_CUDA;
+}
+
+namespace {
+
+bool add_overflows(int64_t a, int64_t b) {
+  return (b > 0 && a > INT64_MAX - b) || (b < 0 && a < INT64_MIN - b);
+}
+
+// Window start and timestamp of iteration `it` (gpu_cpu_temporal_sim.cu:860-902).
+bool slice_start(int64_t start, float step, int64_t window, int32_t it, int64_t &ws,
+                 int64_t &ts) {
+  const double raw = (double)it * (double)step;
+  if (raw > (double)INT64_MAX || raw < (double)INT64_MIN) return false;
+  const int64_t off = (int64_t)llround(raw);
+  if (add_overflows(start, off)) return false;
+  int64_t net = (off / window) * window;
+  if (off < 0 && (off % window)) net -= window;
+  if (add_overflows(start, net)) return false;
+  ws = start + net;
+  ts = start + off;
+  return true;
+}
+
+// Per-step windows, weight scales and timestamps (:859-959).
+rp_status make_schedule(const rp_params &p, std::vector<int64_t> &ws,
+                        std::vector<float> &scale, std::vector<int64_t> &ts) {
+  const int32_t T = p.n_steps;
+  ws.resize(T);
+  scale.resize(T);
+  ts.resize(T);
+  if (p.window <= 0) {
+    set_error("static network duration must be positive");
+    return RP_ERR_ARG;
+  }
+  if (!(p.step_size > 0.0f)) {
+    set_error("step size must be positive");
+    return RP_ERR_ARG;
+  }
+  int64_t cached = 0;
+  bool valid = false;
+  int32_t steps = 1;
+  for (int32_t it = 0; it < T; ++it) {
+    int64_t cs, t;
+    if (!slice_start(p.start_time, p.step_size, p.window, it, cs, t) ||
+        add_overflows(cs, p.window)) {
+      set_error("overflow computing the simulation time of step %d", it);
+      return RP_ERR_RANGE;
+    }
+    if (!valid || cs != cached) {
+      steps = 0;
+      for (int32_t f = it; f < T; ++f) {
+        int64_t fs, ft;
+        if (!slice_start(p.start_time, p.step_size, p.window, f, fs, ft)) {
+          set_error("overflow computing a future simulation time");
+          return RP_ERR_RANGE;
+        }
+        if (fs != cs) break;
+        ++steps;
+      }
+      cached = cs;
+      valid = true;
+    }
+    ws[it] = cs;
+    scale[it] = 1.0f / (float)steps;
+    ts[it] = t;
+  }
+  return RP_OK;
+}
+
+int resolve_path(const rp_params &p) {
+  if (p.path != RP_PATH_AUTO) return p.path;
+  return p.transition == RP_TRANSITION_GEOMETRIC ? RP_PATH_BATCHED : RP_PATH_PLAIN;
+}
+
+}  // namespace
+}  // namespace rp
+
+using namespace rp;
+
+struct rp_sim {
+  const Graph *g = nullptr;
+  rp_params p{};
+  int path = RP_PATH_PLAIN;
+  int weight_kind = kWeightF32;
+  int32_t N = 0, M = 0, T = 0;
+  int64_t cap = 0;
+  std::vector<int64_t> step_ws, step_ts;
+  std::vector<float> step_scale;
+  std::vector<int32_t> step_win;  // window index per step
+  std::vector<WinDesc> wins;
+  std::vector<CandRange> ranges;
+  WindowWorkspace wsp;
+  bool prebuilt = false;
+  std::vector<int64_t> arena_rp_off, arena_ent_off;
+  DevBuf arena_rp, arena_ent;
+  int64_t prebuilt_nnz = 0;
+  // plain state
+  DevBuf state, exposure;
+  // batched state
+  DevBuf sa, sb, mask[2], tasks, ev, rs, init_counts;
+  PackedLayout L{};
+  bool wide_acc = false;
+  DevBuf net_size, net_first, net_rows;
+  int32_t n_nets = 1;
+  // shared
+  DevBuf counts, beta_r, sus, classes;
+  StepConsts c{};
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int kernels_per_run = 0;
+  int64_t nnz_total = 0;
+
+  ~rp_sim() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  const int32_t *rp_of(int t) const {
+    if (prebuilt) return arena_rp.as<int32_t>() + arena_rp_off[step_win[t]];
+    return wsp.row_ptr.as<int32_t>();
+  }
+  const int2 *ent_of(int t) const {
+    if (prebuilt) return arena_ent.as<int2>() + arena_ent_off[step_win[t]];
+    return wsp.entries.as<int2>();
+  }
+
+  // Optional event marks around kernel groups (rp_sim_profile).
+  struct Marks {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;  // group kind of the interval ending at ev[i]
+    cudaStream_t st;
+    void mark(int k) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      cudaEventRecord(e, st);
+      ev.push_back(e);
+      kind.push_back(k);
+    }
+    ~Marks() {
+      for (auto e : ev) cudaEventDestroy(e);
+    }
+  };
+  enum { kMarkStart = 0, kMarkOther = 1, kMarkBuild = 2, kMarkSpmv = 3, kMarkStep = 4 };
+
+  // Enqueues one whole replay.  With `cb`, per-step node states are copied
+  // out and handed to the callback (not capturable).
+  rp_status enqueue(cudaStream_t st, rp_state_cb cb, void *user, int *n_kernels,
+                    Marks *mk = nullptr) {
+    int k = 0;
+    auto mark = [&](int kind) {
+      if (mk) mk->mark(kind);
+    };
+    mark(kMarkStart);
+    const int32_t rows = T + 1;
+    std::vector<uint8_t> host_states;
+    if (cb) host_states.resize((size_t)N * M);
+    auto emit_states = [&](int32_t step_index, int64_t tstamp) -> rp_status {
+      if (!cb) return RP_OK;
+      if (path == RP_PATH_BATCHED)
+        packed_classify(L, sa.as<uint32_t>(), sb.as<uint32_t>(), classes.as<uint8_t>(), st);
+      else
+        plain_classify(p.transition, state.ptr, N, M, classes.as<uint8_t>(), c, st);
+      RP_TRY_CUDA(cudaMemcpyAsync(host_states.data(), classes.ptr, host_states.size(),
+                                  cudaMemcpyDeviceToHost, st));
+      RP_TRY_CUDA(cudaStreamSynchronize(st));
+      if (cb(user, step_index, tstamp, host_states.data(), N, M) != 0) {
+        set_error("state callback aborted the run");
+        return RP_ERR_ARG;
+      }
+      return RP_OK;
+    };
+    if (path == RP_PATH_PLAIN) {
+      RP_TRY_CUDA(cudaMemsetAsync(counts.ptr, 0, counts.bytes, st));
+      plain_init(p.transition, state.ptr, N, M, p.initial_infected, p.initial_count, c, st);
+      plain_count(p.transition, state.ptr, N, M, counts.as<int32_t>(), c, st);
+      k += 2 + (p.initial_count > 0);
+    } else {
+      RP_TRY_CUDA(cudaMemsetAsync(ev.ptr, 0, ev.bytes, st));
+      if (rs.ptr && p.p_rs > 0.0f) RP_TRY_CUDA(cudaMemsetAsync(rs.ptr, 0, rs.bytes, st));
+      RP_TRY_CUDA(cudaMemsetAsync(init_counts.ptr, 0, init_counts.bytes, st));
+      packed_init(L, sa.as<uint32_t>(), sb.as<uint32_t>(), mask[0].as<uint32_t>(),
+                  p.initial_infected, p.initial_count, nullptr, net_first.as<int32_t>(),
+                  net_rows.as<int32_t>(), n_nets, c, st);
+      packed_count(L, tasks.as<PackedTask>(), sa.as<uint32_t>(), sb.as<uint32_t>(),
+                   init_counts.as<unsigned long long>(), st);
+      k += 2 + 2 * (p.initial_count > 0);
+    }
+    mark(kMarkOther);
+    RP_TRY(emit_states(0, p.start_time));
+    const int per_row = n_nets * M;
+    for (int32_t t = 0; t < T; ++t) {
+      const int w = step_win[t];
+      if (!prebuilt && (t == 0 || w != step_win[t - 1])) {
+        enqueue_window_build(*g, wsp, w, wins[w], cap, weight_kind,
+                             weight_kind == kWeightF32, st);
+        k += 5 + (wins[w].may_truncate ? 1 : 0) + (weight_kind == kWeightF32 ? 2 : 0);
+        mark(kMarkBuild);
+      }
+      if (path == RP_PATH_PLAIN) {
+        plain_spmv(p.transition, rp_of(t), ent_of(t), state.ptr, exposure.ptr, N, M, c, st);
+        mark(kMarkSpmv);
+        plain_transition(p.transition, state.ptr, exposure.ptr, N, M, (uint32_t)t,
+                         step_scale[t], counts.as<int32_t>() + (int64_t)(t + 1) * M * 4, c,
+                         st);
+        mark(kMarkStep);
+        k += 2;
+      } else {
+        packed_step(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t),
+                    mask[t & 1].as<uint32_t>(), mask[(t + 1) & 1].as<uint32_t>(),
+                    sa.as<uint32_t>(), sb.as<uint32_t>(),
+                    ev.as<unsigned long long>() + (int64_t)t * per_row,
+                    p.p_rs > 0.0f ? rs.as<unsigned long long>() + (int64_t)t * per_row
+                                  : nullptr,
+                    (uint32_t)t, step_scale[t], wide_acc, c, st);
+        mark(kMarkStep);
+        k += 1;
+      }
+      RP_TRY(emit_states(t + 1, step_ts[t]));
+    }
+    if (path == RP_PATH_BATCHED) {
+      packed_finalize_events(init_counts.as<unsigned long long>(),
+                             ev.as<unsigned long long>(),
+                             p.p_rs > 0.0f ? rs.as<unsigned long long>() : nullptr, T,
+                             per_row, net_size.as<int32_t>(), M, p.has_exposed, p.ir_to_s,
+                             counts.as<int32_t>(), st);
+      k += 1;
+      mark(kMarkOther);
+    }
+    (void)rows;
+    RP_TRY_CUDA(cudaGetLastError());
+    if (n_kernels) *n_kernels = k;
+    return RP_OK;
+  }
+};
+
+namespace {
+
+// Builds every window's canonical CSR once into the arena.
+rp_status prebuild(rp_sim &s) {
+  const int nw = (int)s.wins.size();
+  const int32_t N = s.N;
+  std::vector<int64_t> nnz(nw, 0);
+  DevBuf tmp_rp, tmp_ent;
+  RP_TRY(tmp_rp.alloc(sizeof(int32_t) * ((size_t)N + 1)));
+  RP_TRY(tmp_ent.alloc(sizeof(int2) * (size_t)s.wsp.cap_entries));
+  cudaStream_t st = s.stream;
+  for (int w = 0; w < nw; ++w) {
+    enqueue_window_build(*s.g, s.wsp, w, s.wins[w], s.cap, s.weight_kind, true, st);
+    enqueue_window_compact(s.wsp, tmp_rp.as<int32_t>(), tmp_ent.as<int2>(), st);
+    int32_t total = 0;
+    RP_TRY_CUDA(cudaMemcpyAsync(&total, tmp_rp.as<int32_t>() + N, sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, st));
+    RP_TRY_CUDA(cudaStreamSynchronize(st));
+    nnz[w] = total;
+  }
+  s.arena_rp_off.resize(nw);
+  s.arena_ent_off.resize(nw);
+  int64_t ent = 0;
+  for (int w = 0; w < nw; ++w) {
+    s.arena_rp_off[w] = (int64_t)w * (N + 1);
+    s.arena_ent_off[w] = ent;
+    ent += nnz[w];
+  }
+  s.prebuilt_nnz = ent;
+  RP_TRY(s.arena_rp.alloc(sizeof(int32_t) * (size_t)nw * ((size_t)N + 1)));
+  RP_TRY(s.arena_ent.alloc(sizeof(int2) * (size_t)(ent > 0 ? ent : 1)));
+  for (int w = 0; w < nw; ++w) {
+    enqueue_window_build(*s.g, s.wsp, w, s.wins[w], s.cap, s.weight_kind, true, st);
+    enqueue_window_compact(s.wsp, s.arena_rp.as<int32_t>() + s.arena_rp_off[w],
+                           s.arena_ent.as<int2>() + s.arena_ent_off[w], st);
+  }
+  RP_TRY_CUDA(cudaStreamSynchronize(st));
+  return RP_OK;
+}
+
+rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
+  s.g = &g;
+  s.p = p;
+  s.N = g.n_nodes;
+  s.M = p.n_replicas;
+  s.T = p.n_steps;
+  if (s.M <= 0 || s.T < 0) {
+    set_error("n_replicas must be positive and n_steps non-negative");
+    return RP_ERR_ARG;
+  }
+  if (p.transition != RP_TRANSITION_COUNTDOWN && p.transition != RP_TRANSITION_GEOMETRIC) {
+    set_error("unknown transition mode %d", p.transition);
+    return RP_ERR_ARG;
+  }
+  s.path = resolve_path(p);
+  if (s.path != RP_PATH_PLAIN && s.path != RP_PATH_BATCHED) {
+    set_error("unknown path %d", p.path);
+    return RP_ERR_ARG;
+  }
+  if (s.path == RP_PATH_BATCHED && p.transition == RP_TRANSITION_COUNTDOWN) {
+    set_error("countdown transitions run on the plain path");
+    return RP_ERR_ARG;
+  }
+  if (p.initial_count > s.N) {
+    set_error("initial_count %d exceeds the %d nodes", p.initial_count, s.N);
+    return RP_ERR_ARG;
+  }
+  if (s.path == RP_PATH_PLAIN && (int64_t)s.M > 4 * 65535) {
+    set_error("the plain path supports at most 262140 replicas");
+    return RP_ERR_RANGE;
+  }
+  if (s.path == RP_PATH_BATCHED && s.N >= (1 << 21)) {
+    set_error("batched path counts networks of fewer than 2^21 nodes");
+    return RP_ERR_RANGE;
+  }
+  s.weight_kind = p.transition == RP_TRANSITION_COUNTDOWN ? kWeightF32 : kWeightI32;
+  if (s.weight_kind == kWeightI32 && p.window > INT32_MAX) {
+    set_error("integer contact-second weights need a window of at most 2^31-1 s");
+    return RP_ERR_RANGE;
+  }
+  RP_TRY_CUDA(cudaSetDevice(g.device));
+  RP_TRY_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+
+  // ---- schedule and windows ----
+  RP_TRY(make_schedule(p, s.step_ws, s.step_scale, s.step_ts));
+  s.cap = p.ncls_cap ? (g.nlists > 0 ? g.nlists : 1) : INT64_MAX;
+  s.step_win.resize(s.T);
+  int64_t max_cand = 0;
+  for (int32_t t = 0; t < s.T; ++t) {
+    if (t == 0 || s.step_ws[t] != s.step_ws[t - 1]) {
+      WinDesc d{};
+      plan_window(g, s.step_ws[t], s.step_ws[t] + p.window, s.step_scale[t], s.cap, s.ranges,
+                  d);
+      s.wins.push_back(d);
+      if (d.n_candidates > max_cand) max_cand = d.n_candidates;
+    }
+    s.step_win[t] = (int32_t)s.wins.size() - 1;
+  }
+  if (max_cand > (int64_t)INT32_MAX / 2) {
+    set_error("a window has %lld candidate contacts; at most 2^30 are supported",
+              (long long)max_cand);
+    return RP_ERR_RANGE;
+  }
+  RP_TRY(window_workspace_alloc(s.wsp, s.N, max_cand, (int64_t)s.wins.size(), s.wins,
+                                s.ranges));
+  // Integer accumulators: row sums are bounded by window * entries per row.
+  s.wide_acc = (double)p.window * (double)(2 * max_cand) >= 2147483647.0;
+
+  // ---- constants ----
+  s.c.key0 = (uint32_t)p.seed;
+  s.c.key1 = (uint32_t)(p.seed >> 32);
+  s.c.step_size = p.step_size;
+  s.c.neg_log_base = -logf(1.0f - p.infect_prob);
+  s.c.E = p.exposed_duration;
+  s.c.I = p.infectious_duration;
+  s.c.R = p.resistant_duration;
+  s.c.upper = p.exposed_duration + p.infectious_duration + p.resistant_duration;
+  s.c.medium = p.infectious_duration + p.resistant_duration;
+  s.c.lower = p.resistant_duration;
+  s.c.p_ei = p.p_ei;
+  s.c.p_ir = p.p_ir;
+  s.c.p_rs = p.p_rs;
+  s.c.has_exposed = p.has_exposed;
+  s.c.ir_to_s = p.ir_to_s;
+  s.c.beta = p.beta;
+  if (p.beta_per_replica) {
+    RP_TRY(s.beta_r.alloc(sizeof(float) * s.M));
+    RP_TRY_CUDA(cudaMemcpy(s.beta_r.ptr, p.beta_per_replica, sizeof(float) * s.M,
+                           cudaMemcpyHostToDevice));
+    s.c.beta_r = s.beta_r.as<float>();
+  }
+  if (p.susceptibility) {
+    RP_TRY(s.sus.alloc(sizeof(float) * (size_t)s.N));
+    RP_TRY_CUDA(cudaMemcpy(s.sus.ptr, p.susceptibility, sizeof(float) * s.N,
+                           cudaMemcpyHostToDevice));
+    s.c.sus = s.sus.as<float>();
+  }
+  return RP_OK;
+}
+
+// Rows per batched task, by graph size: enough tasks for every SM to hold
+// two CTAs, each task long enough to amortise its count flush.
+int32_t rows_per_task(int32_t n_rows, int32_t n_slices, int32_t rg) {
+  const int64_t target_tasks = 148 * 2 * 4;
+  int64_t rows = ((int64_t)n_rows * n_slices + target_tasks - 1) / target_tasks;
+  const int64_t quantum = 8 * rg;
+  if (rows < quantum) rows = quantum;
+  if (rows > 8192) rows = 8192;
+  rows = (rows + quantum - 1) / quantum * quantum;
+  return (int32_t)rows;
+}
+
+rp_status alloc_state(rp_sim &s) {
+  const int32_t N = s.N, M = s.M, T = s.T;
+  const int64_t NM = (int64_t)N * M;
+  RP_TRY(s.counts.alloc(sizeof(int32_t) * (size_t)(T + 1) * (size_t)M * 4 * s.n_nets));
+  if (s.p.record_node_states) RP_TRY(s.classes.alloc((size_t)NM));
+  if (s.path == RP_PATH_PLAIN) {
+    const size_t sb = s.p.transition == RP_TRANSITION_COUNTDOWN ? 4 : 1;
+    const size_t eb = s.p.transition == RP_TRANSITION_COUNTDOWN ? 4 : 8;
+    RP_TRY(s.state.alloc(sb * (size_t)NM));
+    RP_TRY(s.exposure.alloc(eb * (size_t)NM));
+    return RP_OK;
+  }
+  // batched layout
+  PackedLayout &L = s.L;
+  L.n_nodes = N;
+  L.m = M;
+  L.words = (M + 31) / 32;
+  int ws = 1;
+  while (ws < L.words && ws < 32) ws <<= 1;
+  L.ws = ws;
+  L.last_mask = (M % 32) ? ((1u << (M % 32)) - 1u) : 0xFFFFFFFFu;
+  const int32_t n_slices = (L.words + ws - 1) / ws;
+  const int32_t rg = 32 / ws;
+  std::vector<PackedTask> tasks;
+  std::vector<int32_t> first, rows, size;
+  // single network: rows [0, N)
+  first.push_back(0);
+  rows.push_back(N);
+  size.push_back(N);
+  for (int net = 0; net < s.n_nets; ++net) {
+    const int32_t rpt = rows_per_task(rows[net], n_slices, rg);
+    for (int32_t r0 = first[net]; r0 < first[net] + rows[net]; r0 += rpt)
+      for (int32_t sl = 0; sl < n_slices; ++sl)
+        tasks.push_back(PackedTask{r0, std::min(r0 + rpt, first[net] + rows[net]), sl,
+                                   net * M});
+  }
+  L.n_tasks = (int32_t)tasks.size();
+  L.counts_stride = s.n_nets * M;
+  const size_t plane = sizeof(uint32_t) * (size_t)N * L.words;
+  RP_TRY(s.sa.alloc(plane));
+  RP_TRY(s.sb.alloc(plane));
+  RP_TRY(s.mask[0].alloc(plane));
+  RP_TRY(s.mask[1].alloc(plane));
+  RP_TRY(s.tasks.alloc(sizeof(PackedTask) * tasks.size()));
+  RP_TRY_CUDA(cudaMemcpy(s.tasks.ptr, tasks.data(), sizeof(PackedTask) * tasks.size(),
+                         cudaMemcpyHostToDevice));
+  const size_t per_row = (size_t)s.n_nets * M;
+  RP_TRY(s.ev.alloc(sizeof(unsigned long long) * per_row * (size_t)(T > 0 ? T : 1)));
+  if (s.p.p_rs > 0.0f)
+    RP_TRY(s.rs.alloc(sizeof(unsigned long long) * per_row * (size_t)(T > 0 ? T : 1)));
+  RP_TRY(s.init_counts.alloc(sizeof(unsigned long long) * per_row));
+  RP_TRY(s.net_first.alloc(sizeof(int32_t) * first.size()));
+  RP_TRY(s.net_rows.alloc(sizeof(int32_t) * rows.size()));
+  RP_TRY(s.net_size.alloc(sizeof(int32_t) * size.size()));
+  RP_TRY_CUDA(cudaMemcpy(s.net_first.ptr, first.data(), sizeof(int32_t) * first.size(),
+                         cudaMemcpyHostToDevice));
+  RP_TRY_CUDA(cudaMemcpy(s.net_rows.ptr, rows.data(), sizeof(int32_t) * rows.size(),
+                         cudaMemcpyHostToDevice));
+  RP_TRY_CUDA(cudaMemcpy(s.net_size.ptr, size.data(), sizeof(int32_t) * size.size(),
+                         cudaMemcpyHostToDevice));
+  return RP_OK;
+}
+
+rp_status capture(rp_sim &s) {
+  cudaGraph_t graph = nullptr;
+  RP_TRY_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
+  rp_status st = s.enqueue(s.stream, nullptr, nullptr, &s.kernels_per_run);
+  cudaError_t e = cudaStreamEndCapture(s.stream, &graph);
+  if (st != RP_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&s.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+  return RP_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+RP_API const char *rp_last_error(void) { return g_err; }
+RP_API const char *rp_version(void) { return "replay-b200 0.1 (sm_100a)"; }
+
+RP_API rp_status rp_graph_load_text(const char *path, int device, rp_graph **out) {
+  if (!path || !out) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  *out = nullptr;
+  std::unique_ptr<rp_graph> h(new rp_graph());
+  std::vector<int64_t> st, en;
+  std::vector<int32_t> u, v;
+  int32_t n_nodes = 0, n_index = 0;
+  int64_t malformed = 0;
+  RP_TRY(parse_contact_file(path, n_nodes, n_index, malformed, st, en, u, v));
+  h->g.device = device;
+  h->g.n_index = n_index;
+  h->g.n_malformed = malformed;
+  RP_TRY(graph_build(h->g, st, en, u, v, n_nodes));
+  *out = h.release();
+  return RP_OK;
+}
+
+RP_API rp_status rp_graph_from_arrays(const int64_t *start, const int64_t *end,
+                                      const int32_t *u, const int32_t *v, int64_t n_contacts,
+                                      int32_t n_nodes, int device, rp_graph **out) {
+  if (!out || n_contacts < 0 || n_nodes <= 0 ||
+      (n_contacts > 0 && (!start || !end || !u || !v))) {
+    set_error("invalid graph arrays");
+    return RP_ERR_ARG;
+  }
+  *out = nullptr;
+  std::vector<int64_t> st(start, start + n_contacts), en(end, end + n_contacts);
+  std::vector<int32_t> uu(n_contacts), vv(n_contacts);
+  std::vector<uint8_t> seen(n_nodes, 0);
+  int32_t n_index = 0;
+  for (int64_t k = 0; k < n_contacts; ++k) {
+    if (u[k] < 0 || v[k] < 0 || u[k] >= n_nodes || v[k] >= n_nodes) {
+      set_error("contact %lld joins node outside [0, %d)", (long long)k, n_nodes);
+      return RP_ERR_ARG;
+    }
+    uu[k] = u[k] < v[k] ? u[k] : v[k];
+    vv[k] = u[k] < v[k] ? v[k] : u[k];
+    n_index += !seen[u[k]];
+    seen[u[k]] = 1;
+    n_index += !seen[v[k]];
+    seen[v[k]] = 1;
+  }
+  std::unique_ptr<rp_graph> h(new rp_graph());
+  h->g.device = device;
+  h->g.n_index = n_index;
+  RP_TRY(graph_build(h->g, st, en, uu, vv, n_nodes));
+  *out = h.release();
+  return RP_OK;
+}
+
+RP_API rp_status rp_graph_get_info(const rp_graph *h, rp_graph_info *o) {
+  if (!h || !o) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  const Graph &g = h->g;
+  o->n_nodes = g.n_nodes;
+  o->n_index = g.n_index;
+  o->n_contacts = g.n_contacts;
+  o->nlists = g.nlists;
+  o->n_malformed = g.n_malformed;
+  o->t_min = g.t_min;
+  o->t_max = g.t_max;
+  o->n_classes = g.n_classes_used;
+  o->device = g.device;
+  return RP_OK;
+}
+
+RP_API void rp_graph_free(rp_graph *h) { delete h; }
+
+RP_API rp_status rp_window_csr(rp_graph *h, int64_t ws, int64_t we, float scale,
+                               int32_t weight_kind, int32_t ncls_cap, int32_t *row_ptr,
+                               int32_t *col, void *val, int64_t capacity, int64_t *nnz,
+                               int64_t *n_hits) {
+  if (!h || !row_ptr || !nnz || !n_hits || we <= ws ||
+      (weight_kind != kWeightF32 && weight_kind != kWeightI32)) {
+    set_error("invalid window CSR request");
+    return RP_ERR_ARG;
+  }
+  const Graph &g = h->g;
+  if (weight_kind == kWeightI32 && we - ws > INT32_MAX) {
+    set_error("integer weights need a window of at most 2^31-1 s");
+    return RP_ERR_RANGE;
+  }
+  RP_TRY_CUDA(cudaSetDevice(g.device));
+  const int64_t cap = ncls_cap ? (g.nlists > 0 ? g.nlists : 1) : INT64_MAX;
+  std::vector<WinDesc> wins(1);
+  std::vector<CandRange> ranges;
+  plan_window(g, ws, we, scale, cap, ranges, wins[0]);
+  WindowWorkspace w;
+  RP_TRY(window_workspace_alloc(w, g.n_nodes, wins[0].n_candidates, 1, wins, ranges));
+  DevBuf out_rp, out_ent;
+  RP_TRY(out_rp.alloc(sizeof(int32_t) * ((size_t)g.n_nodes + 1)));
+  RP_TRY(out_ent.alloc(sizeof(int2) * (size_t)w.cap_entries));
+  cudaStream_t st = nullptr;
+  enqueue_window_build(g, w, 0, wins[0], cap, weight_kind, true, st);
+  unsigned long long hits_raw = 0;
+  RP_TRY_CUDA(cudaMemcpyAsync(&hits_raw, w.counters.as<unsigned long long>() + 3,
+                              sizeof(hits_raw), cudaMemcpyDeviceToHost, st));
+  enqueue_window_compact(w, out_rp.as<int32_t>(), out_ent.as<int2>(), st);
+  RP_TRY_CUDA(cudaMemcpyAsync(row_ptr, out_rp.ptr, sizeof(int32_t) * ((size_t)g.n_nodes + 1),
+                              cudaMemcpyDeviceToHost, st));
+  RP_TRY_CUDA(cudaStreamSynchronize(st));
+  const int64_t total = row_ptr[g.n_nodes];
+  *nnz = total;
+  *n_hits = (int64_t)hits_raw < cap ? (int64_t)hits_raw : cap;
+  if (total > capacity) {
+    set_error("CSR has %lld entries, capacity %lld", (long long)total, (long long)capacity);
+    return RP_ERR_RANGE;
+  }
+  if (total > 0) {
+    std::vector<int2> ent((size_t)total);
+    RP_TRY_CUDA(cudaMemcpy(ent.data(), out_ent.ptr, sizeof(int2) * (size_t)total,
+                           cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < total; ++k) {
+      if (col) col[k] = ent[k].x;
+      if (val) static_cast<int32_t *>(val)[k] = ent[k].y;
+    }
+  }
+  return RP_OK;
+}
+
+RP_API void rp_params_default(rp_params *p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->struct_size = sizeof(rp_params);
+  p->n_replicas = 1000;
+  p->n_steps = 42;
+  p->step_size = 3600.0f;
+  p->start_time = 946713600;
+  p->window = 3600;
+  p->transition = RP_TRANSITION_COUNTDOWN;
+  p->path = RP_PATH_AUTO;
+  p->csr_mode = RP_CSR_PER_STEP;
+  p->ncls_cap = 1;
+  p->seed = 1;
+  p->has_exposed = 1;
+}
+
+RP_API rp_status rp_sim_create(const rp_graph *h, const rp_params *p, rp_sim **out) {
+  if (!h || !p || !out) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  if (p->struct_size != sizeof(rp_params)) {
+    set_error("rp_params.struct_size mismatch (%u, expected %zu)", p->struct_size,
+              sizeof(rp_params));
+    return RP_ERR_ARG;
+  }
+  *out = nullptr;
+  std::unique_ptr<rp_sim> s(new rp_sim());
+  RP_TRY(sim_setup(*s, h->g, *p));
+  RP_TRY(alloc_state(*s));
+  s->prebuilt = p->csr_mode == RP_CSR_PREBUILT;
+  if (s->prebuilt) RP_TRY(prebuild(*s));
+  for (int32_t t = 0; t < s->T; ++t) {
+    // nnz multiplied per step (for the roofline); per-step mode counts the
+    // candidate bound, replaced by exact values when prebuilt.
+    if (s->prebuilt) {
+      const int w = s->step_win[t];
+      const int64_t next = (w + 1 < (int)s->wins.size()) ? s->arena_ent_off[w + 1]
+                                                         : s->prebuilt_nnz;
+      s->nnz_total += next - s->arena_ent_off[w];
+    }
+  }
+  if (!p->record_node_states) RP_TRY(capture(*s));
+  *out = s.release();
+  return RP_OK;
+}
+
+RP_API void rp_sim_free(rp_sim *s) { delete s; }
+
+RP_API rp_status rp_sim_enqueue(rp_sim *s, void *stream) {
+  if (!s) {
+    set_error("null simulation");
+    return RP_ERR_ARG;
+  }
+  RP_TRY_CUDA(cudaSetDevice(s->g->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (s->exec) {
+    RP_TRY_CUDA(cudaGraphLaunch(s->exec, st));
+    return RP_OK;
+  }
+  return s->enqueue(st, nullptr, nullptr, nullptr);
+}
+
+RP_API rp_status rp_sim_counts(rp_sim *s, int32_t *counts) {
+  if (!s || !counts) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  RP_TRY_CUDA(cudaSetDevice(s->g->device));
+  RP_TRY_CUDA(cudaDeviceSynchronize());
+  RP_TRY_CUDA(cudaMemcpy(counts, s->counts.ptr, s->counts.bytes, cudaMemcpyDeviceToHost));
+  return RP_OK;
+}
+
+RP_API rp_status rp_sim_run(rp_sim *s, int32_t *counts, rp_state_cb cb, void *user) {
+  if (!s || !counts) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  RP_TRY_CUDA(cudaSetDevice(s->g->device));
+  if (s->p.record_node_states && cb) {
+    RP_TRY(s->enqueue(s->stream, cb, user, nullptr));
+  } else if (s->exec) {
+    RP_TRY_CUDA(cudaGraphLaunch(s->exec, s->stream));
+  } else {
+    RP_TRY(s->enqueue(s->stream, nullptr, nullptr, nullptr));
+  }
+  RP_TRY_CUDA(cudaMemcpyAsync(counts, s->counts.ptr, s->counts.bytes, cudaMemcpyDeviceToHost,
+                              s->stream));
+  RP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  return RP_OK;
+}
+
+RP_API rp_status rp_sim_timestamps(rp_sim *s, int64_t *ts) {
+  if (!s || !ts) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  ts[0] = s->p.start_time;
+  for (int32_t t = 0; t < s->T; ++t) ts[t + 1] = s->step_ts[t];
+  return RP_OK;
+}
+
+RP_API rp_status rp_sim_get_info(const rp_sim *s, rp_sim_info *o) {
+  if (!s || !o) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  o->path = s->path;
+  o->words = s->path == RP_PATH_BATCHED ? s->L.words : 0;
+  o->n_windows = (int32_t)s->wins.size();
+  o->kernels_per_run = s->kernels_per_run;
+  int64_t mc = 0;
+  for (auto &w : s->wins) mc = w.n_candidates > mc ? w.n_candidates : mc;
+  o->max_candidates = mc;
+  o->prebuilt_nnz = s->prebuilt_nnz;
+  int64_t bytes = 0;
+  const DevBuf *bufs[] = {&s->arena_rp, &s->arena_ent, &s->state, &s->exposure, &s->sa,
+                          &s->sb, &s->mask[0], &s->mask[1], &s->tasks, &s->ev, &s->rs,
+                          &s->init_counts, &s->counts, &s->beta_r, &s->sus, &s->classes,
+                          &s->wsp.hits, &s->wsp.entries, &s->wsp.erank, &s->wsp.tmp_e,
+                          &s->wsp.tmp_r, &s->wsp.row_ptr, &s->wsp.deg, &s->wsp.tiles,
+                          &s->wsp.long_rows};
+  for (auto b : bufs) bytes += (int64_t)b->bytes;
+  o->device_bytes = bytes;
+  o->nnz_total = s->nnz_total;
+  return RP_OK;
+}
+
+RP_API rp_status rp_sim_profile(rp_sim *s, rp_profile *out) {
+  if (!s || !out) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  RP_TRY_CUDA(cudaSetDevice(s->g->device));
+  RP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  rp_sim::Marks mk;
+  mk.st = s->stream;
+  int nk = 0;
+  RP_TRY(s->enqueue(s->stream, nullptr, nullptr, &nk, &mk));
+  RP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  memset(out, 0, sizeof(*out));
+  for (size_t i = 1; i < mk.ev.size(); ++i) {
+    float ms = 0.0f;
+    RP_TRY_CUDA(cudaEventElapsedTime(&ms, mk.ev[i - 1], mk.ev[i]));
+    out->total_ms += ms;
+    switch (mk.kind[i]) {
+      case rp_sim::kMarkBuild: out->build_ms += ms; out->build_launches++; break;
+      case rp_sim::kMarkSpmv: out->spmv_ms += ms; out->spmv_launches++; break;
+      case rp_sim::kMarkStep: out->step_ms += ms; out->step_launches++; break;
+      default: out->other_ms += ms; break;
+    }
+  }
+  out->kernels = nk;
+  return RP_OK;
+}
+
+RP_API rp_status rp_exposure_spmv_f32(const int32_t *d_row_ptr, const int32_t *d_col,
+                                      const float *d_val, int32_t n_nodes,
+                                      const float *d_infectious, float *d_exposure,
+                                      int32_t n_replicas, void *stream) {
+  if (!d_row_ptr || n_nodes <= 0 || n_replicas <= 0 || !d_infectious || !d_exposure) {
+    set_error("invalid SpMV arguments");
+    return RP_ERR_ARG;
+  }
+  plain_spmv_f32_raw(d_row_ptr, d_col, d_val, n_nodes, d_infectious, d_exposure, n_replicas,
+                     static_cast<cudaStream_t>(stream));
+  RP_TRY_CUDA(cudaGetLastError());
+  return RP_OK;
+}
+
+RP_API rp_status rp_exposure_spmm_packed(const int32_t *d_row_ptr, const int32_t *d_entries,
+                                         int32_t n_nodes, const uint32_t *d_masks,
+                                         int32_t words, int32_t n_replicas,
+                                         int64_t *d_exposure, void *stream) {
+  if (!d_row_ptr || n_nodes <= 0 || n_replicas <= 0 || words != (n_replicas + 31) / 32 ||
+      !d_masks || !d_exposure) {
+    set_error("invalid packed SpMM arguments");
+    return RP_ERR_ARG;
+  }
+  packed_exposure(d_row_ptr, reinterpret_cast<const int2 *>(d_entries), n_nodes, d_masks,
+                  words, n_replicas, d_exposure, static_cast<cudaStream_t>(stream));
+  RP_TRY_CUDA(cudaGetLastError());
+  return RP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+// Device helpers shared by the replay kernels (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rp {
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): 10 rounds of two
+// 32x32->64 multiplies with a Weyl key schedule.  Counter-based: every
+// (key, counter) pair is an independent draw, so any thread can produce the
+// uniform of any (replica, node, step) without state.
+__device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1,
+                                              uint32_t c2, uint32_t c3,
+                                              uint32_t k0, uint32_t k1,
+                                              uint32_t out[4]) {
+#pragma unroll
+  for (int round = 0; round < 10; ++round) {
+    const uint32_t lo0 = 0xD2511F53u * c0;
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2);
+    const uint32_t n0 = hi1 ^ c1 ^ k0;
+    const uint32_t n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
+// Uniform on the 24-bit grid ((x >> 8) + 1) * 2^-24, in (0, 1]; exact in
+// float, so host and device agree bit for bit.
+__device__ __forceinline__ float unit24(uint32_t x) {
+  return __fmul_rn(__uint2float_rn((x >> 8) + 1u), 0x1p-24f);
+}
+
+// Random stream layout: key = seed; counter = (node, step, replica / 4,
+// stream); output word replica % 4.  Stream 0 drives the per-step
+// transitions, stream 1 the Bernoulli initial condition (step 0xFFFFFFFF),
+// stream 2 the exact-count initial condition (node = draw index,
+// step 0xFFFFFFFE, third word = replica).
+constexpr uint32_t kStreamStep = 0u;
+constexpr uint32_t kStreamInit = 1u;
+constexpr uint32_t kStreamPick = 2u;
+constexpr uint32_t kStepInit = 0xFFFFFFFFu;
+constexpr uint32_t kStepPick = 0xFFFFFFFEu;
+
+// 1 - exp(-x) for x >= 0 from correctly rounded multiplies and adds only
+// (no FMA contraction): Cody-Waite reduction x = k ln2 + r with ln2 split in
+// a 15-bit head and a tail, then the Taylor series of expm1(-r) through
+// r^9/9! in Horner form.  Max error about 1 ulp; NaN propagates (the
+// reference's p = 1, zero-exposure case), +inf gives 1.
+__device__ __forceinline__ float one_minus_exp_neg(float x) {
+  if (x != x) return x;
+  if (!(x > 0.0f)) return 0.0f;
+  if (x >= 87.0f) return 1.0f;
+  const float inv_ln2 = 0x1.715476p+0f;
+  const float ln2_hi = 0x1.62e4p-1f;
+  const float ln2_lo = 0x1.7f7d1cp-20f;
+  const int k = __float2int_rz(__fadd_rn(__fmul_rn(x, inv_ln2), 0.5f));
+  const float kf = __int2float_rn(k);
+  const float r =
+      __fsub_rn(__fsub_rn(x, __fmul_rn(kf, ln2_hi)), __fmul_rn(kf, ln2_lo));
+  const float y = -r;
+  float p = 0x1.71de3ap-19f;
+  p = __fadd_rn(__fmul_rn(p, y), 0x1.a01a02p-16f);
+  p = __fadd_rn(__fmul_rn(p, y), 0x1.a01a02p-13f);
+  p = __fadd_rn(__fmul_rn(p, y), 0x1.6c16c2p-10f);
+  p = __fadd_rn(__fmul_rn(p, y), 0x1.111112p-7f);
+  p = __fadd_rn(__fmul_rn(p, y), 0x1.555556p-5f);
+  p = __fadd_rn(__fmul_rn(p, y), 0x1.555556p-3f);
+  p = __fadd_rn(__fmul_rn(p, y), 0.5f);
+  const float em1 = __fadd_rn(y, __fmul_rn(__fmul_rn(y, y), p));
+  if (k == 0) return -em1;
+  const float scale = __int_as_float((127 - k) << 23);
+  const float e = __fmul_rn(__fadd_rn(1.0f, em1), scale);
+  return __fsub_rn(1.0f, e);
+}
+
+// Countdown arithmetic of the reference (int op float, truncated back to
+// int): c = (int)((float)c - step) and c = (int)((float)base + step).
+__device__ __forceinline__ int32_t cd_sub(int32_t c, float step) {
+  return __float2int_rz(__fsub_rn(__int2float_rn(c), step));
+}
+__device__ __forceinline__ int32_t cd_add(int32_t base, float step) {
+  return __float2int_rz(__fadd_rn(__int2float_rn(base), step));
+}
+
+// Summary classification of a countdown value
+// (tool/gpu_cpu_temporal_sim.cu:530-550): 0 S, 1 E, 2 I, 3 R.
+__device__ __forceinline__ int countdown_class(int32_t c, int32_t E, int32_t I,
+                                               int32_t R) {
+  const int32_t upper = E + I + R;
+  const int32_t elapsed = (c <= 0 || c > upper) ? 0 : (upper - c);
+  if (c == 0) return 0;
+  if (E > 0 && elapsed < E) return 1;
+  if (I > 0 && elapsed < E + I) return 2;
+  if (R > 0 && elapsed < E + I + R) return 3;
+  return 0;
+}
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+}  // namespace rp

@@ -1,0 +1,229 @@
+// Internal types shared by the host driver and the kernel translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/replay.h"
+
+namespace rp {
+
+// ---- errors ---------------------------------------------------------------
+void set_error(const char *fmt, ...);
+rp_status cuda_fail(cudaError_t e, const char *what);
+#define RP_TRY_CUDA(call)                                  \
+  do {                                                     \
+    cudaError_t _e = (call);                               \
+    if (_e != cudaSuccess) return ::rp::cuda_fail(_e, #call); \
+  } while (0)
+#define RP_TRY(call)                 \
+  do {                               \
+    rp_status _s = (call);           \
+    if (_s != RP_OK) return _s;      \
+  } while (0)
+
+// ---- device buffer ----------------------------------------------------------
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  rp_status alloc(size_t n) {
+    release();
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      (void)cudaGetLastError();
+      set_error("cudaMalloc of %zu bytes failed: %s", n, cudaGetErrorString(e));
+      return RP_ERR_NOMEM;
+    }
+    bytes = n;
+    return RP_OK;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T *as() const {
+    return static_cast<T *>(ptr);
+  }
+};
+
+// ---- interval index -----------------------------------------------------------
+// Contacts live in "stored coordinates" (the reference interval database's
+// orientation rule, see graph.cpp) and are partitioned into duration classes:
+// class 0 holds durations <= 1 s (including empty and inverted intervals),
+// class c >= 1 holds durations in (2^(c-1), 2^c].  Inside a class contacts
+// are ordered by start, so the candidates of a query [qs, qe) in class c are
+// the contiguous run with start in (qs - 2^c, qe): two binary searches.
+constexpr int kClasses = 64;
+
+struct CandRange {
+  int64_t lo;     // first candidate, index into the class-ordered arrays
+  int64_t count;  // candidates in this class
+  int64_t prefix; // candidates in earlier ranges of the same window
+};
+
+struct WinDesc {
+  int64_t ws, we;        // window [ws, we)
+  int64_t qs, qe;        // query actually run (mirrored when ws < 0)
+  int64_t n_candidates;  // sum of range counts
+  float scale;           // 1 / steps in the window (reference weight scale)
+  int32_t range_off;     // first CandRange of this window
+  int32_t n_ranges;
+  int32_t may_truncate;  // candidates exceed the hit cap
+};
+
+struct Graph {
+  int device = 0;
+  int32_t n_nodes = 0, n_index = 0;
+  int64_t n_contacts = 0, nlists = 0, n_malformed = 0;
+  int64_t t_min = 0, t_max = 0;
+  int32_t n_classes_used = 0;
+  std::vector<int64_t> class_off;  // kClasses + 1 offsets
+  std::vector<int64_t> h_cs;       // class-ordered stored starts
+  DevBuf cs, ce;                   // int64 stored start / end, class order
+  DevBuf cu, cv;                   // int32 endpoints (u <= v)
+  DevBuf crank;                    // int32 position in (start asc, end desc) order
+};
+
+rp_status parse_contact_file(const char *path, int32_t &n_nodes,
+                             int32_t &n_index, int64_t &n_malformed,
+                             std::vector<int64_t> &start,
+                             std::vector<int64_t> &end, std::vector<int32_t> &u,
+                             std::vector<int32_t> &v);
+rp_status graph_build(Graph &g, std::vector<int64_t> &start,
+                      std::vector<int64_t> &end, std::vector<int32_t> &u,
+                      std::vector<int32_t> &v, int32_t n_nodes);
+
+// Plans the query of one window: candidate ranges appended to `ranges`.
+void plan_window(const Graph &g, int64_t ws, int64_t we, float scale,
+                 int64_t cap, std::vector<CandRange> &ranges, WinDesc &out);
+
+// ---- window builder ----------------------------------------------------------
+struct Hit {
+  int32_t rank;  // position in (start asc, end desc) order
+  int32_t u;     // < 0: counts toward the hit cap but carries no weight
+  int32_t v;
+  int32_t w;     // int32 seconds or float bits
+};
+
+struct WindowWorkspace {
+  int32_t n_nodes = 0;
+  int64_t cap_hits = 0, cap_entries = 0;
+  int32_t n_tiles = 0;
+  DevBuf hits;      // Hit[cap_hits]
+  DevBuf entries;   // int2 {col, weight}[cap_entries]
+  DevBuf erank;     // int32[cap_entries]
+  DevBuf tmp_e;     // int2[cap_entries]  radix ping-pong for hub rows
+  DevBuf tmp_r;     // int32[cap_entries]
+  DevBuf row_ptr;   // int32[n+1]
+  DevBuf deg;       // int32[n] degree, then fill cursor
+  DevBuf tiles;     // int32[n_tiles]
+  DevBuf counters;  // u64[4]: recorded hits, long rows, spare, predicate hits
+  DevBuf long_rows; // int32[n]
+  DevBuf win;       // WinDesc[n_windows]
+  DevBuf ranges;    // CandRange[...]
+};
+
+rp_status window_workspace_alloc(WindowWorkspace &w, int32_t n_nodes,
+                                 int64_t cap_hits, int64_t n_windows,
+                                 const std::vector<WinDesc> &wins,
+                                 const std::vector<CandRange> &ranges);
+
+enum WeightKind { kWeightF32 = 0, kWeightI32 = 1 };
+
+// Enqueues the CSR build of window `wi` into ws.row_ptr / ws.entries.
+// sort_rows: order each row by (col, rank) and merge duplicates in place
+// (merged-away entries keep their column with weight 0).
+void enqueue_window_build(const Graph &g, WindowWorkspace &ws, int wi,
+                          const WinDesc &desc, int64_t cap, int weight_kind,
+                          bool sort_rows, cudaStream_t st);
+// Compacts the sorted, merged CSR in ws into (row_ptr_out, entries_out):
+// drops merged-away entries.  tmp_rows: int32[n+1] scratch.
+void enqueue_window_compact(WindowWorkspace &ws, int32_t *row_ptr_out,
+                            int2 *entries_out, cudaStream_t st);
+
+// ---- kernels of the step loop -------------------------------------------------
+struct StepConsts {
+  uint32_t key0, key1;
+  float step_size;
+  float neg_log_base;  // -logf(1 - infect_prob), countdown mode
+  int32_t upper, medium, lower, E, I, R;  // countdown ranges / durations
+  float p_ei, p_ir, p_rs;
+  int32_t has_exposed, ir_to_s;
+  float beta;
+  const float *beta_r;  // device, may be null
+  const float *sus;     // device, may be null
+};
+
+// Plain path (column-major N x M state, per-replica SpMV + elementwise).
+void plain_init(int transition, void *state, int32_t n, int32_t m,
+                float p0, int32_t k_exact, const StepConsts &c,
+                cudaStream_t st);
+void plain_spmv(int transition, const int32_t *row_ptr, const int2 *entries,
+                const void *state, void *exposure, int32_t n, int32_t m,
+                const StepConsts &c, cudaStream_t st);
+void plain_transition(int transition, void *state, const void *exposure,
+                      int32_t n, int32_t m, uint32_t step, float scale,
+                      int32_t *counts_row, const StepConsts &c,
+                      cudaStream_t st);
+void plain_count(int transition, const void *state, int32_t n, int32_t m,
+                 int32_t *counts_row, const StepConsts &c, cudaStream_t st);
+void plain_classify(int transition, const void *state, int32_t n, int32_t m,
+                    uint8_t *out, const StepConsts &c, cudaStream_t st);
+
+// Batched path (bit-packed replica words).
+struct PackedTask {
+  int32_t row_begin, row_end;  // rows of one network
+  int32_t slice;               // 32-word slice (or the only slice)
+  int32_t count_base;          // index of replica 0 of this network in counts
+};
+struct PackedLayout {
+  int32_t n_nodes, words, m;  // m: replicas per network
+  int32_t ws;                 // words per row group (1..32, power of 2)
+  uint32_t last_mask;         // valid bits of the last word
+  int32_t n_tasks;
+  int32_t counts_stride;      // u64 entries per count row
+};
+void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb,
+                 uint32_t *mask, float p0, int32_t k_exact,
+                 const int32_t *net_of_row, const int32_t *net_first_row,
+                 const int32_t *net_rows, int32_t n_nets,
+                 const StepConsts &c, cudaStream_t st);
+void packed_step(const PackedLayout &L, const PackedTask *tasks,
+                 const int32_t *row_ptr, const int2 *entries,
+                 const uint32_t *mask_in, uint32_t *mask_out, uint32_t *sa,
+                 uint32_t *sb, unsigned long long *ev_row,
+                 unsigned long long *rs_row, uint32_t step, float scale,
+                 bool wide_acc, const StepConsts &c, cudaStream_t st);
+void packed_count(const PackedLayout &L, const PackedTask *tasks,
+                  const uint32_t *sa, const uint32_t *sb,
+                  unsigned long long *counts_row, cudaStream_t st);
+void packed_finalize_events(const unsigned long long *init,
+                            const unsigned long long *ev,
+                            const unsigned long long *rs, int32_t steps,
+                            int32_t per_row, const int32_t *net_size,
+                            int32_t m, int32_t has_exposed, int32_t ir_to_s,
+                            int32_t *counts, cudaStream_t st);
+void packed_classify(const PackedLayout &L, const uint32_t *sa,
+                     const uint32_t *sb, uint8_t *out, cudaStream_t st);
+void packed_exposure(const int32_t *row_ptr, const int2 *entries, int32_t n,
+                     const uint32_t *masks, int32_t words, int32_t m,
+                     int64_t *exposure, cudaStream_t st);
+void plain_spmv_f32_raw(const int32_t *row_ptr, const int32_t *col,
+                        const float *val, int32_t n, const float *b, float *c,
+                        int32_t m, cudaStream_t st);
+
+}  // namespace rp
+
+struct rp_graph {
+  rp::Graph g;
+};
