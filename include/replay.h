@@ -215,6 +215,9 @@ typedef struct {
   int32_t kernels;         /* all kernel launches of the replay */
 } rp_profile;
 RP_API rp_status rp_sim_profile(rp_sim *s, rp_profile *out);
+/* Device time of each step's exposure + transition kernels (n_steps floats,
+ * ms) from the same eager replay; no reference counterpart. */
+RP_API rp_status rp_sim_profile_steps(rp_sim *s, float *step_ms);
 
 /* ------------------------------------------------------------------------ */
 /* Kernel test hooks on device pointers.                                     */

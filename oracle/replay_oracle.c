@@ -78,6 +78,38 @@ float orc_uniform(uint64_t seed, uint32_t node, uint32_t step,
   return orc_unit(out[replica & 3u]);
 }
 
+/* Fixed-point threshold floor(p * 2^64) of a per-step probability, with
+ * p >= 1 flagged as certain. */
+uint64_t orc_threshold64(float p, int *always) {
+  *always = p >= 1.0f;
+  if (!(p > 0.0f) || p >= 1.0f) return 0;
+  return (uint64_t)ldexp((double)p, 64);
+}
+
+/* Flow decision of replica r (E->I, I->R, R->S): its per-step uniform U is
+ * bit (r % 32) of successive random planes; plane k (k = 0 is 2^-1) is
+ * output k % 4 of Philox(key = seed, counter = (node, step, r / 32,
+ * (k / 4) << 4)).  Event iff U < T on the first 64 bits. */
+int orc_flow_event(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica,
+                   uint64_t T, int always) {
+  if (always) return 1;
+  if (T == 0) return 0;
+  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  const uint32_t bit = replica & 31u;
+  for (int j = 0; j < 16; j++) {
+    uint32_t ctr[4] = {node, step, replica >> 5, (uint32_t)j << 4};
+    uint32_t x[4];
+    orc_philox4x32_10(ctr, key, x);
+    for (int q = 0; q < 4; q++) {
+      const int k = 4 * j + q;
+      const uint32_t wb = (x[q] >> bit) & 1u;
+      const uint32_t tb = (uint32_t)(T >> (63 - k)) & 1u;
+      if (wb != tb) return wb < tb;
+    }
+  }
+  return 0;
+}
+
 /* 1 - exp(-x) for x >= 0 using only correctly rounded +,-,*: Cody-Waite
  * reduction x = k ln2 + r, |r| <= ln2/2, and the Taylor series of expm1(-r)
  * through r^9/9!.  The device code performs the identical sequence with
@@ -753,8 +785,10 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
                 Rd = p->resistant_duration;
   const int32_t upper = Ed + Id + Rd, medium = Id + Rd, lower = Rd;
   const float neg_log_base = -logf(1.0f - p->infect_prob);
-  const uint32_t key0 = (uint32_t)p->seed;
-  (void)key0;
+  int te_all, ti_all, tr_all;
+  const uint64_t te = orc_threshold64(p->p_ei, &te_all);
+  const uint64_t ti = orc_threshold64(p->p_ir, &ti_all);
+  const uint64_t tr = orc_threshold64(p->p_rs, &tr_all);
 
   /* initial state */
   if (p->initial_count > 0 && p->initial_count > N) {
@@ -811,7 +845,7 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
           if (cd[idx] == 0) {
             float e = expf_[idx] / 3600.0f;
             float P = orc_one_minus_exp_neg(neg_log_base * e);
-            float uu = orc_uniform(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, 0u);
+            float uu = orc_uniform(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, 3u);
             if (P > uu) cd[idx] = (int32_t)((float)upper + p->step_size);
           }
         }
@@ -828,7 +862,6 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
         for (int32_t i = 0; i < N; i++) {
           int64_t idx = i + (int64_t)r * N;
           int32_t st = cd[idx];
-          float uu = orc_uniform(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, 0u);
           if (st == 0) {
             if (expi[idx] > 0) {
               float sus = p->susceptibility ? p->susceptibility[i] : 1.0f;
@@ -836,14 +869,18 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
               float ef = (float)expi[idx];
               if (scale[t] != 1.0f) ef = ef * scale[t];
               float P = orc_one_minus_exp_neg(bs * ef);
+              float uu = orc_uniform(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, 3u);
               if (P > uu) cd[idx] = p->has_exposed ? 1 : 2;
             }
           } else if (st == 1) {
-            if (uu < p->p_ei) cd[idx] = 2;
+            if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, te, te_all))
+              cd[idx] = 2;
           } else if (st == 2) {
-            if (uu < p->p_ir) cd[idx] = p->ir_to_s ? 0 : 3;
+            if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, ti, ti_all))
+              cd[idx] = p->ir_to_s ? 0 : 3;
           } else {
-            if (p->p_rs > 0.0f && uu < p->p_rs) cd[idx] = 0;
+            if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, tr, tr_all))
+              cd[idx] = 0;
           }
         }
       }

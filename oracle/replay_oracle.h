@@ -20,13 +20,24 @@
 extern "C" {
 #endif
 
-/* ---- counter-based random numbers ---------------------------------------- */
+/* ---- counter-based random numbers ---------------------------------------- *
+ * key = seed; counter = (node, step, c2, c3):
+ *   infection (S->E, S->I) uniform of replica r: c2 = r / 4, c3 = 3, output
+ *     r % 4, as the 24-bit grid value ((x >> 8) + 1) 2^-24; event iff P > u;
+ *   flow (E->I, I->R, R->S) uniform of replica r: bit-sliced, see
+ *     orc_flow_event;
+ *   initial Bernoulli: step = 0xFFFFFFFF, c2 = r / 4, c3 = 1;
+ *   initial exact count (Floyd): node = draw j, step = 0xFFFFFFFE, c2 = r,
+ *     c3 = 2. */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2],
                        uint32_t out[4]);
 float orc_unit(uint32_t x); /* ((x>>8)+1) * 2^-24, in (0,1] */
 float orc_uniform(uint64_t seed, uint32_t node, uint32_t step,
                   uint32_t replica, uint32_t stream);
 float orc_one_minus_exp_neg(float x);
+uint64_t orc_threshold64(float p, int *always);
+int orc_flow_event(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica,
+                   uint64_t T, int always);
 
 /* ---- ingest ---------------------------------------------------------------- */
 int64_t orc_timegm(int year, int month0, int mday, int hour, int min, int sec);

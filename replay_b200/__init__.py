@@ -175,6 +175,12 @@ class Simulation:
         check(lib().rp_sim_profile(self._h, C.byref(pr)))
         return {k: getattr(pr, k) for k, _ in pr._fields_}
 
+    def profile_steps(self):
+        """Per-step device time (ms) of the exposure + transition kernels."""
+        ms = np.zeros(max(self.T, 1), np.float32)
+        check(lib().rp_sim_profile_steps(self._h, _ptr(ms)))
+        return ms[: self.T]
+
     def enqueue(self, stream=None):
         """Enqueues the whole replay on a CUDA stream handle (int) without sync."""
         check(lib().rp_sim_enqueue(self._h, C.c_void_p(stream) if stream else None))

@@ -129,9 +129,8 @@ struct rp_sim {
   // plain state
   DevBuf state, exposure;
   // batched state
-  DevBuf sa, sb, mask[2], tasks, ev, rs, init_counts;
+  DevBuf sa, sb, mask[2], evs, tasks, ev, rs, init_counts;
   PackedLayout L{};
-  bool wide_acc = false;
   DevBuf net_size, net_first, net_rows;
   int32_t n_nets = 1;
   // shared
@@ -211,7 +210,7 @@ struct rp_sim {
       if (rs.ptr && p.p_rs > 0.0f) RP_TRY_CUDA(cudaMemsetAsync(rs.ptr, 0, rs.bytes, st));
       RP_TRY_CUDA(cudaMemsetAsync(init_counts.ptr, 0, init_counts.bytes, st));
       packed_init(L, sa.as<uint32_t>(), sb.as<uint32_t>(), mask[0].as<uint32_t>(),
-                  p.initial_infected, p.initial_count, nullptr, net_first.as<int32_t>(),
+                  p.initial_infected, p.initial_count, net_first.as<int32_t>(),
                   net_rows.as<int32_t>(), n_nets, c, st);
       packed_count(L, tasks.as<PackedTask>(), sa.as<uint32_t>(), sb.as<uint32_t>(),
                    init_counts.as<unsigned long long>(), st);
@@ -239,13 +238,13 @@ struct rp_sim {
       } else {
         packed_step(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t),
                     mask[t & 1].as<uint32_t>(), mask[(t + 1) & 1].as<uint32_t>(),
-                    sa.as<uint32_t>(), sb.as<uint32_t>(),
+                    sa.as<uint32_t>(), sb.as<uint32_t>(), evs.as<uint32_t>(),
                     ev.as<unsigned long long>() + (int64_t)t * per_row,
                     p.p_rs > 0.0f ? rs.as<unsigned long long>() + (int64_t)t * per_row
                                   : nullptr,
-                    (uint32_t)t, step_scale[t], wide_acc, c, st);
+                    (uint32_t)t, step_scale[t], c, st);
         mark(kMarkStep);
-        k += 1;
+        k += 2;
       }
       RP_TRY(emit_states(t + 1, step_ts[t]));
     }
@@ -370,8 +369,6 @@ rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
   }
   RP_TRY(window_workspace_alloc(s.wsp, s.N, max_cand, (int64_t)s.wins.size(), s.wins,
                                 s.ranges));
-  // Integer accumulators: row sums are bounded by window * entries per row.
-  s.wide_acc = (double)p.window * (double)(2 * max_cand) >= 2147483647.0;
 
   // ---- constants ----
   s.c.key0 = (uint32_t)p.seed;
@@ -384,6 +381,14 @@ rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
   s.c.upper = p.exposed_duration + p.infectious_duration + p.resistant_duration;
   s.c.medium = p.infectious_duration + p.resistant_duration;
   s.c.lower = p.resistant_duration;
+  auto thr = [](float pr, int &all) -> unsigned long long {
+    all = pr >= 1.0f;
+    if (!(pr > 0.0f) || pr >= 1.0f) return 0ull;
+    return (unsigned long long)ldexp((double)pr, 64);
+  };
+  s.c.th.te = thr(p.p_ei, s.c.th.te_all);
+  s.c.th.ti = thr(p.p_ir, s.c.th.ti_all);
+  s.c.th.tr = thr(p.p_rs, s.c.th.tr_all);
   s.c.p_ei = p.p_ei;
   s.c.p_ir = p.p_ir;
   s.c.p_rs = p.p_rs;
@@ -429,17 +434,19 @@ rp_status alloc_state(rp_sim &s) {
     RP_TRY(s.exposure.alloc(eb * (size_t)NM));
     return RP_OK;
   }
-  // batched layout
+  // batched layout: rows padded to 4-word columns, 32 columns per slice
   PackedLayout &L = s.L;
   L.n_nodes = N;
   L.m = M;
-  L.words = (M + 31) / 32;
-  int ws = 1;
-  while (ws < L.words && ws < 32) ws <<= 1;
-  L.ws = ws;
+  L.vwords = (M + 31) / 32;
+  L.words = (L.vwords + 3) / 4 * 4;
+  L.q4 = L.words / 4;
   L.last_mask = (M % 32) ? ((1u << (M % 32)) - 1u) : 0xFFFFFFFFu;
-  const int32_t n_slices = (L.words + ws - 1) / ws;
-  const int32_t rg = 32 / ws;
+  int lpr = 1;
+  while (lpr < L.q4 && lpr < 32) lpr <<= 1;
+  L.lpr = lpr;
+  const int32_t n_slices = (L.q4 + 31) / 32;
+  const int32_t rg = 32 / lpr;
   std::vector<PackedTask> tasks;
   std::vector<int32_t> first, rows, size;
   // single network: rows [0, N)
@@ -454,12 +461,12 @@ rp_status alloc_state(rp_sim &s) {
                                    net * M});
   }
   L.n_tasks = (int32_t)tasks.size();
-  L.counts_stride = s.n_nets * M;
   const size_t plane = sizeof(uint32_t) * (size_t)N * L.words;
   RP_TRY(s.sa.alloc(plane));
   RP_TRY(s.sb.alloc(plane));
   RP_TRY(s.mask[0].alloc(plane));
   RP_TRY(s.mask[1].alloc(plane));
+  RP_TRY(s.evs.alloc(plane));
   RP_TRY(s.tasks.alloc(sizeof(PackedTask) * tasks.size()));
   RP_TRY_CUDA(cudaMemcpy(s.tasks.ptr, tasks.data(), sizeof(PackedTask) * tasks.size(),
                          cudaMemcpyHostToDevice));
@@ -750,7 +757,7 @@ RP_API rp_status rp_sim_get_info(const rp_sim *s, rp_sim_info *o) {
   o->prebuilt_nnz = s->prebuilt_nnz;
   int64_t bytes = 0;
   const DevBuf *bufs[] = {&s->arena_rp, &s->arena_ent, &s->state, &s->exposure, &s->sa,
-                          &s->sb, &s->mask[0], &s->mask[1], &s->tasks, &s->ev, &s->rs,
+                          &s->sb, &s->mask[0], &s->mask[1], &s->evs, &s->tasks, &s->ev, &s->rs,
                           &s->init_counts, &s->counts, &s->beta_r, &s->sus, &s->classes,
                           &s->wsp.hits, &s->wsp.entries, &s->wsp.erank, &s->wsp.tmp_e,
                           &s->wsp.tmp_r, &s->wsp.row_ptr, &s->wsp.deg, &s->wsp.tiles,
@@ -786,6 +793,31 @@ RP_API rp_status rp_sim_profile(rp_sim *s, rp_profile *out) {
     }
   }
   out->kernels = nk;
+  return RP_OK;
+}
+
+RP_API rp_status rp_sim_profile_steps(rp_sim *s, float *step_ms) {
+  if (!s || !step_ms) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  RP_TRY_CUDA(cudaSetDevice(s->g->device));
+  RP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  rp_sim::Marks mk;
+  mk.st = s->stream;
+  int nk = 0;
+  RP_TRY(s->enqueue(s->stream, nullptr, nullptr, &nk, &mk));
+  RP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  int t = 0;
+  for (size_t i = 1; i < mk.ev.size(); ++i) {
+    float ms = 0.0f;
+    RP_TRY_CUDA(cudaEventElapsedTime(&ms, mk.ev[i - 1], mk.ev[i]));
+    if (mk.kind[i] == rp_sim::kMarkSpmv && t < s->T) step_ms[t] = ms;
+    if (mk.kind[i] == rp_sim::kMarkStep && t < s->T) {
+      step_ms[t] = (s->path == RP_PATH_PLAIN ? step_ms[t] : 0.0f) + ms;
+      ++t;
+    }
+  }
   return RP_OK;
 }
 

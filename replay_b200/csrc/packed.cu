@@ -1,27 +1,33 @@
-// Batched path: replica-bit-packed state, one fused kernel per step.
+// Batched path: replica-bit-packed state, two kernels per step.
 //
-// Layout in HBM, node-major with replicas packed 32 per uint32 word
-// (words = ceil(M / 32) per node):
+// Layout in HBM, node-major, 32 replicas per uint32 word; every node row is
+// padded to a multiple of 4 words so that a lane moves 128 replicas with one
+// 16-byte access:
 //   sa, sb    state planes; replica bit (a, b): S (0,0), E (0,1), I (1,0),
 //             R (1,1)
-//   mask_t    infectious bits of step t (= a & ~b), double-buffered: step t
-//             reads mask_t of the neighbours and writes mask_{t+1}
-// The CSR of the step's window is {col, weight} pairs (int32 contact-seconds).
+//   mask_t    infectious bits of step t (a & ~b), double-buffered: step t
+//             reads mask_t and writes mask_{t+1}
+//   evs       infection events of the step, written for rows with contacts
+// The window CSR holds {col, weight} pairs (int32 contact-seconds).
 //
-// k_packed_step, per (row, word) lane:
-//   1. read the state planes, decode S/E/I/R masks;
-//   2. exposure: for every neighbour j, m = mask_t[j, word] & S; replicas
-//      with a set bit accumulate the edge weight (exact integer sums, the
-//      replacement of cusparseSpMM, tool/gpu_cpu_temporal_sim.cu:1062);
-//   3. transition: one Philox uniform per replica that can move, keyed
-//      (seed, replica, node, step), same rules and same uniforms as the
-//      plain path's k_transition_geometric;
-//   4. write changed planes and mask_{t+1};
-//   5. count transition events per replica in bit-sliced (vertical)
-//      counters, reduce them per CTA and add them to the step's event row;
-//      counts(t+1) = counts(t) + events(t) is resolved by k_finalize.
-// A warp covers `ws` words of 32/ws rows at a time; a task is a run of rows
-// of one network for one 32-word slice.
+// k_infect (exposure SpMM + infection draws), per row with contacts, lanes
+// over 4-word columns (the replacement of cusparseSpMM,
+// tool/gpu_cpu_temporal_sim.cu:1062, and monte_carlo_simulation, :137-159):
+//   1. inf = OR over neighbours j of mask_t[j] (16 B per lane per entry);
+//   2. exposed = inf & S; the quads (4 replicas) holding exposed replicas are
+//      compacted across the warp so every lane draws: exact int64 exposure
+//      sums of the quad's replicas over the row's entries, one Philox call,
+//      P = 1 - exp(-beta_r s_i e) > u (the replica's infection uniform);
+//   3. events go to evs.
+// k_flow (transitions + count reduction), every (row, 4-word column):
+//   reads the planes and the row's infection events, draws the bit-sliced
+//   flow uniforms of the E, I (and waning R) replicas, 32 replicas per random
+//   plane (flow_events), applies all moves with bitwise operations, writes the
+//   planes and mask_{t+1}, and adds every transition event to per-replica
+//   counters in shared memory, flushed once per task to the step's event
+//   row; k_finalize turns initial counts + events into per-step counts.
+// Every decision uses the state at the start of the step: k_infect reads the
+// planes before k_flow rewrites them.
 #include "rp_device.cuh"
 #include "rp_internal.h"
 
@@ -29,260 +35,309 @@ namespace rp {
 namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
-constexpr int kPlanes = 8;  // vertical counters hold up to 255 events/lane
+constexpr int kFieldBits = 21;  // global event fields: S->E | ->I | I->
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
 
-// Event fields of one u64: S->E | ->I | I-> , 21 bits each.
-constexpr int kFieldBits = 21;
-
-__device__ __forceinline__ void vc_add(uint32_t (&P)[kPlanes], uint32_t m) {
-#pragma unroll
-  for (int k = 0; k < kPlanes; ++k) {
-    const uint32_t t = P[k] & m;
-    P[k] ^= m;
-    m = t;
-    if (!m) break;
-  }
+__device__ __forceinline__ uint32_t word_mask(const PackedLayout &L, int word) {
+  return word < L.vwords - 1 ? kFull : (word == L.vwords - 1 ? L.last_mask : 0u);
 }
 
-__device__ __forceinline__ uint32_t vc_count(const uint32_t (&P)[kPlanes], int r) {
-  uint32_t c = 0;
-#pragma unroll
-  for (int k = 0; k < kPlanes; ++k) c |= ((P[k] >> r) & 1u) << k;
-  return c;
+__device__ __forceinline__ uint32_t get4(const uint4 &v, int w) {
+  return w == 0 ? v.x : (w == 1 ? v.y : (w == 2 ? v.z : v.w));
 }
 
-__device__ __forceinline__ uint32_t vc_any(const uint32_t (&P)[kPlanes]) {
+// 8-bit mask of the non-empty nibbles of x.
+__device__ __forceinline__ uint32_t nibble_any(uint32_t x) {
+  x |= x >> 1;
+  x |= x >> 2;
+  x &= 0x11111111u;
   uint32_t o = 0;
 #pragma unroll
-  for (int k = 0; k < kPlanes; ++k) o |= P[k];
+  for (int q = 0; q < 8; ++q) o |= ((x >> (4 * q)) & 1u) << q;
   return o;
 }
 
-template <int WS>
-__device__ __forceinline__ unsigned long long group_sum(unsigned long long v) {
-  // sum over lanes with the same word offset (lane % WS)
-#pragma unroll
-  for (int o = WS; o < 32; o <<= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
-
-// Flushes the lane's vertical counters into the CTA's shared event rows.
-template <int WS>
-__device__ void flush_events(uint32_t (&cSE)[kPlanes], uint32_t (&cXI)[kPlanes],
-                             uint32_t (&cIX)[kPlanes], uint32_t (&cRS)[kPlanes],
-                             unsigned long long *s_ev, unsigned long long *s_rs,
-                             int wsub, int rsub) {
-  const uint32_t any = vc_any(cSE) | vc_any(cXI) | vc_any(cIX);
-  const uint32_t any_rs = vc_any(cRS);
-  const uint32_t any_w = __reduce_or_sync(kFull, any | any_rs);
-  if (!any_w) return;
-#pragma unroll 1
-  for (int r = 0; r < 32; ++r) {
-    if (!((any_w >> r) & 1u)) continue;
-    unsigned long long v = (unsigned long long)vc_count(cSE, r) |
-                           ((unsigned long long)vc_count(cXI, r) << kFieldBits) |
-                           ((unsigned long long)vc_count(cIX, r) << (2 * kFieldBits));
-    unsigned long long w = vc_count(cRS, r);
-    v = group_sum<WS>(v);
-    w = group_sum<WS>(w);
-    if (rsub == 0) {
-      if (v) atomicAdd(&s_ev[wsub * 32 + r], v);
-      if (w) atomicAdd(&s_rs[wsub * 32 + r], w);
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < kPlanes; ++k) cSE[k] = cXI[k] = cIX[k] = cRS[k] = 0;
-}
-
-template <int WS, typename Acc>
-__global__ void __launch_bounds__(256, 2)
-    k_packed_step(PackedLayout L, const PackedTask *__restrict__ tasks,
-                  const int32_t *__restrict__ row_ptr, const int2 *__restrict__ ent,
-                  const uint32_t *__restrict__ mask_in, uint32_t *__restrict__ mask_out,
-                  uint32_t *__restrict__ sa, uint32_t *__restrict__ sb,
-                  unsigned long long *__restrict__ ev_row,
-                  unsigned long long *__restrict__ rs_row, uint32_t step, float scale,
-                  StepConsts c) {
-  constexpr int RG = 32 / WS;
-  __shared__ unsigned long long s_ev[WS * 32];
-  __shared__ unsigned long long s_rs[WS * 32];
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads)
+    k_infect(PackedLayout L, const PackedTask *__restrict__ tasks,
+             const int32_t *__restrict__ row_ptr, const int2 *__restrict__ ent,
+             const uint4 *__restrict__ mask_in, const uint4 *__restrict__ sa,
+             const uint4 *__restrict__ sb, uint4 *__restrict__ evs, uint32_t step, float scale,
+             StepConsts c) {
+  __shared__ uint32_t s_exp[kWarps][32][4];
+  __shared__ uint32_t s_ev[kWarps][32][4];
+  __shared__ int32_t s_off[kWarps][32];
+  __shared__ uint32_t s_qm[kWarps][32];
+  __shared__ int32_t s_row[kWarps][32];
+  __shared__ int32_t s_col[kWarps][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
-  const int rsub = lane / WS, wsub = lane % WS;
-  const int W = L.words;
+  const int lpr = L.lpr, rpw = 32 / lpr;
+  const int rsub = lane / lpr, csub = lane % lpr;
+  const uint32_t *mask_w = reinterpret_cast<const uint32_t *>(mask_in);
   for (int ti = blockIdx.x; ti < L.n_tasks; ti += gridDim.x) {
     const PackedTask T = tasks[ti];
-    for (int j = threadIdx.x; j < WS * 32; j += blockDim.x) {
-      s_ev[j] = 0;
-      s_rs[j] = 0;
-    }
-    __syncthreads();
-    const int word = T.slice * WS + wsub;
-    const bool word_ok = word < W;
-    const uint32_t vmask = word_ok ? (word == W - 1 ? L.last_mask : kFull) : 0u;
-    uint32_t cSE[kPlanes], cXI[kPlanes], cIX[kPlanes], cRS[kPlanes];
-#pragma unroll
-    for (int k = 0; k < kPlanes; ++k) cSE[k] = cXI[k] = cIX[k] = cRS[k] = 0;
-    int ev_rows = 0;
-    for (int base = T.row_begin + warp * RG; base < T.row_end; base += nwarps * RG) {
+    const int cbase = T.slice * 32;
+    const int ncols = min(32, L.q4 - cbase);
+    for (int base = T.row_begin + warp * rpw; base < T.row_end; base += kWarps * rpw) {
       const int row = base + rsub;
-      const bool active = word_ok && row < T.row_end;
-      uint32_t tSE = 0, tXI = 0, tIX = 0, tRS = 0;
-      if (active) {
-        const int64_t idx = (int64_t)row * W + word;
-        const uint32_t a = sa[idx], b = sb[idx];
-        const uint32_t S = ~a & ~b & vmask, E = ~a & b, I = a & ~b, R = a & b;
-        Acc acc[32];
-#pragma unroll
-        for (int r = 0; r < 32; ++r) acc[r] = 0;
-        uint32_t exposed = 0;
-        if (S) {
-          const int32_t beg = row_ptr[row], end = row_ptr[row + 1];
-          for (int32_t k = beg; k < end; ++k) {
-            const int2 en = ent[k];
-            const uint32_t mm = mask_in[(int64_t)en.x * W + word] & S;
-            if (mm) {
-              exposed |= mm;
-#pragma unroll
-              for (int r = 0; r < 32; ++r) acc[r] += ((mm >> r) & 1u) ? (Acc)en.y : (Acc)0;
-            }
+      const bool row_ok = row < T.row_end;
+      int32_t beg = 0, end = 0;
+      if (row_ok) {
+        beg = row_ptr[row];
+        end = row_ptr[row + 1];
+      }
+      const bool nonempty = row_ok && end > beg;
+      // ---- OR of the neighbours' infectious words, 4 columns per lane ----
+      // (warp-uniform trip count: the compaction below shuffles)
+      for (int cc0 = 0; cc0 < ncols; cc0 += lpr) {
+        const int cc = cc0 + csub;
+        const bool col_ok = cc < ncols;
+        const int col = cbase + (col_ok ? cc : 0);
+        uint4 inf = make_uint4(0, 0, 0, 0);
+        if (nonempty && col_ok) {
+          int32_t k = beg;
+          for (; k + 2 <= end; k += 2) {
+            const int2 e0 = ent[k], e1 = ent[k + 1];
+            const uint4 m0 = mask_in[(int64_t)e0.x * L.q4 + col];
+            const uint4 m1 = mask_in[(int64_t)e1.x * L.q4 + col];
+            inf.x |= m0.x | m1.x;
+            inf.y |= m0.y | m1.y;
+            inf.z |= m0.z | m1.z;
+            inf.w |= m0.w | m1.w;
+          }
+          if (k < end) {
+            const int2 e0 = ent[k];
+            const uint4 m0 = mask_in[(int64_t)e0.x * L.q4 + col];
+            inf.x |= m0.x;
+            inf.y |= m0.y;
+            inf.z |= m0.z;
+            inf.w |= m0.w;
           }
         }
-        const uint32_t need = exposed | E | I | (c.p_rs > 0.0f ? R : 0u);
-        uint32_t na = a, nb = b;
-        if (need) {
-          const float sus = c.sus ? c.sus[row] : 1.0f;
+        uint32_t ex[4] = {0, 0, 0, 0};
+        if (inf.x | inf.y | inf.z | inf.w) {
+          const int64_t idx = (int64_t)row * L.q4 + col;
+          const uint4 a = sa[idx], b = sb[idx];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            if ((need >> (4 * q)) & 0xFu) {
-              uint32_t x[4];
-              philox4x32_10((uint32_t)row, step, (uint32_t)(word * 8 + q), kStreamStep,
-                            c.key0, c.key1, x);
+          for (int w = 0; w < 4; ++w)
+            ex[w] = get4(inf, w) & ~get4(a, w) & ~get4(b, w) & word_mask(L, 4 * col + w);
+        }
+        uint32_t qm = 0;
 #pragma unroll
-              for (int cc = 0; cc < 4; ++cc) {
-                const int r = 4 * q + cc;
-                const uint32_t bit = 1u << r;
-                if (!(need & bit)) continue;
-                const float u = unit24(x[cc]);
-                if (S & bit) {
-                  const float br = c.beta_r ? c.beta_r[word * 32 + r] : c.beta;
-                  const float bs = c.sus ? __fmul_rn(br, sus) : br;
-                  float ef = (sizeof(Acc) == 8) ? __ll2float_rn((long long)acc[r])
-                                                : __int2float_rn((int)acc[r]);
-                  if (scale != 1.0f) ef = __fmul_rn(ef, scale);
-                  const float P = one_minus_exp_neg(__fmul_rn(bs, ef));
-                  if (P > u) {
-                    if (c.has_exposed)
-                      nb |= bit;
-                    else
-                      na |= bit;
-                  }
-                } else if (E & bit) {
-                  if (u < c.p_ei) {
-                    na |= bit;
-                    nb &= ~bit;
-                  }
-                } else if (I & bit) {
-                  if (u < c.p_ir) {
-                    if (c.ir_to_s)
-                      na &= ~bit;
-                    else
-                      nb |= bit;
-                  }
-                } else {
-                  if (u < c.p_rs) {
-                    na &= ~bit;
-                    nb &= ~bit;
-                  }
-                }
+        for (int w = 0; w < 4; ++w) qm |= nibble_any(ex[w]) << (8 * w);
+        // ---- compact the exposed quads of the warp ----
+        const int cnt = __popc(qm);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(kFull, incl, 31);
+        if (total) {
+          s_off[warp][lane] = incl - cnt;
+          s_qm[warp][lane] = qm;
+          s_row[warp][lane] = row;
+          s_col[warp][lane] = col;
+#pragma unroll
+          for (int w = 0; w < 4; ++w) {
+            s_exp[warp][lane][w] = ex[w];
+            s_ev[warp][lane][w] = 0;
+          }
+          __syncwarp();
+          for (int p = lane; p < total; p += 32) {
+            int owner = 0;
+#pragma unroll
+            for (int st = 16; st > 0; st >>= 1)
+              if (owner + st < 32 && s_off[warp][owner + st] <= p) owner += st;
+            uint32_t m = s_qm[warp][owner];
+            for (int k = p - s_off[warp][owner]; k > 0; --k) m &= m - 1;
+            const int slot = __ffs(m) - 1;
+            const int w = slot >> 3, q = slot & 7;
+            const int orow = s_row[warp][owner];
+            const int word = 4 * s_col[warp][owner] + w;
+            const uint32_t bits = (s_exp[warp][owner][w] >> (4 * q)) & 0xFu;
+            long long e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+            const int32_t ob = row_ptr[orow], oe = row_ptr[orow + 1];
+            for (int32_t k = ob; k < oe; ++k) {
+              const int2 en = ent[k];
+              const uint32_t mw = mask_w[(int64_t)en.x * L.words + word] >> (4 * q);
+              e0 += (mw & 1u) ? en.y : 0;
+              e1 += (mw & 2u) ? en.y : 0;
+              e2 += (mw & 4u) ? en.y : 0;
+              e3 += (mw & 8u) ? en.y : 0;
+            }
+            uint32_t x[4];
+            philox4x32_10((uint32_t)orow, step, (uint32_t)(word * 8 + q), kStreamInfect, c.key0,
+                          c.key1, x);
+            const float sus = c.sus ? c.sus[orow] : 1.0f;
+            const long long ev4[4] = {e0, e1, e2, e3};
+            uint32_t ev = 0;
+#pragma unroll
+            for (int cq = 0; cq < 4; ++cq) {
+              if ((bits >> cq) & 1u) {
+                const int r = word * 32 + 4 * q + cq;
+                const float br = c.beta_r ? c.beta_r[r] : c.beta;
+                const float bs = c.sus ? __fmul_rn(br, sus) : br;
+                float ef = __ll2float_rn(ev4[cq]);
+                if (scale != 1.0f) ef = __fmul_rn(ef, scale);
+                if (one_minus_exp_neg(__fmul_rn(bs, ef)) > unit24(x[cq]))
+                  ev |= 1u << (4 * q + cq);
               }
             }
+            if (ev) atomicOr(&s_ev[warp][owner][w], ev);
           }
-          const uint32_t nI = na & ~nb;
-          tSE = S & ~na & nb;
-          tXI = (S | E) & nI;
-          tIX = I & ~nI;
-          tRS = R & ~na & ~nb;
-          if (na != a) sa[idx] = na;
-          if (nb != b) sb[idx] = nb;
+          __syncwarp();
+#pragma unroll
+          for (int w = 0; w < 4; ++w) ex[w] = s_ev[warp][lane][w];
+          __syncwarp();
         }
-        mask_out[idx] = na & ~nb;
-      }
-      if (tSE | tXI | tIX | tRS) {
-        if (tSE) vc_add(cSE, tSE);
-        if (tXI) vc_add(cXI, tXI);
-        if (tIX) vc_add(cIX, tIX);
-        if (tRS) vc_add(cRS, tRS);
-        ++ev_rows;
-      }
-      if (__any_sync(kFull, ev_rows == (1 << kPlanes) - 1)) {
-        flush_events<WS>(cSE, cXI, cIX, cRS, s_ev, s_rs, wsub, rsub);
-        ev_rows = 0;
+        if (nonempty && col_ok)
+          evs[(int64_t)row * L.q4 + col] = make_uint4(ex[0], ex[1], ex[2], ex[3]);
       }
     }
-    flush_events<WS>(cSE, cXI, cIX, cRS, s_ev, s_rs, wsub, rsub);
+  }
+}
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void count_bits(unsigned long long *s_ev, int wl, uint32_t t,
+                                           unsigned long long inc) {
+  while (t) {
+    const int r = __ffs(t) - 1;
+    atomicAdd(&s_ev[wl * 32 + r], inc);
+    t &= t - 1;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_flow(PackedLayout L, const PackedTask *__restrict__ tasks,
+           const int32_t *__restrict__ row_ptr, const uint4 *__restrict__ evs,
+           uint4 *__restrict__ mask_out, uint4 *__restrict__ sa, uint4 *__restrict__ sb,
+           unsigned long long *__restrict__ ev_row, unsigned long long *__restrict__ rs_row,
+           uint32_t step, StepConsts c) {
+  // per task: 128 words x 32 replicas of 4 x 16-bit event counters
+  __shared__ unsigned long long s_ev[128 * 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lpr = L.lpr, rpw = 32 / lpr;
+  const int rsub = lane / lpr, csub = lane % lpr;
+  const bool waning = c.th.tr_all || c.th.tr != 0;
+  const unsigned long long kSE = 1ull, kXI = 1ull << 16, kIX = 1ull << 32, kRS = 1ull << 48;
+  for (int ti = blockIdx.x; ti < L.n_tasks; ti += gridDim.x) {
+    const PackedTask T = tasks[ti];
+    const int cbase = T.slice * 32;
+    const int ncols = min(32, L.q4 - cbase);
+    for (int j = threadIdx.x; j < 128 * 32; j += blockDim.x) s_ev[j] = 0;
     __syncthreads();
-    for (int j = threadIdx.x; j < WS * 32; j += blockDim.x) {
-      const int rep = (T.slice * WS + (j >> 5)) * 32 + (j & 31);
+    for (int base = T.row_begin + warp * rpw; base < T.row_end; base += kWarps * rpw) {
+      const int row = base + rsub;
+      if (row >= T.row_end) continue;
+      const bool nonempty = row_ptr[row + 1] > row_ptr[row];
+      for (int cc = csub; cc < ncols; cc += lpr) {
+        const int col = cbase + cc;
+        const int64_t idx = (int64_t)row * L.q4 + col;
+        const uint4 a4 = sa[idx], b4 = sb[idx];
+        const uint4 e4 = nonempty ? evs[idx] : make_uint4(0, 0, 0, 0);
+        uint32_t na[4], nb[4], mo[4];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const int word = 4 * col + w;
+          const uint32_t a = get4(a4, w), b = get4(b4, w);
+          na[w] = a;
+          nb[w] = b;
+          mo[w] = 0;
+          if (!word_mask(L, word)) continue;
+          const uint32_t E = ~a & b, I = a & ~b, R = a & b;
+          const uint32_t evS = get4(e4, w);
+          const uint32_t Rw = waning ? R : 0u;
+          const uint32_t evF =
+              (E | I | Rw) ? flow_events(E, I, Rw, c.th, c.key0, c.key1, (uint32_t)row, step,
+                                         (uint32_t)word)
+                           : 0u;
+          const uint32_t evE = evF & E, evI = evF & I, evR = evF & Rw;
+          uint32_t xa = a, xb = b;
+          if (c.has_exposed)
+            xb |= evS;
+          else
+            xa |= evS;
+          xa |= evE;
+          xb &= ~evE;
+          if (c.ir_to_s)
+            xa &= ~evI;
+          else
+            xb |= evI;
+          xa &= ~evR;
+          xb &= ~evR;
+          na[w] = xa;
+          nb[w] = xb;
+          mo[w] = xa & ~xb;
+          const int wl = 4 * cc + w;
+          if (evS | evE | evI | evR) {
+            count_bits(s_ev, wl, c.has_exposed ? evS : 0u, kSE);
+            count_bits(s_ev, wl, evE | (c.has_exposed ? 0u : evS), kXI);
+            count_bits(s_ev, wl, evI, kIX);
+            count_bits(s_ev, wl, evR, kRS);
+          }
+        }
+        const uint4 oa = make_uint4(na[0], na[1], na[2], na[3]);
+        const uint4 ob = make_uint4(nb[0], nb[1], nb[2], nb[3]);
+        if (oa.x != a4.x || oa.y != a4.y || oa.z != a4.z || oa.w != a4.w) sa[idx] = oa;
+        if (ob.x != b4.x || ob.y != b4.y || ob.z != b4.z || ob.w != b4.w) sb[idx] = ob;
+        mask_out[idx] = make_uint4(mo[0], mo[1], mo[2], mo[3]);
+      }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x) {
+      const unsigned long long v = s_ev[j];
+      if (!v) continue;
+      const int rep = cbase * 128 + j;
       if (rep >= L.m) continue;
-      if (s_ev[j]) atomicAdd(&ev_row[T.count_base + rep], s_ev[j]);
-      if (rs_row && s_rs[j]) atomicAdd(&rs_row[T.count_base + rep], s_rs[j]);
+      const unsigned long long f = 0xFFFFull;
+      const unsigned long long g = (v & f) | (((v >> 16) & f) << kFieldBits) |
+                                   (((v >> 32) & f) << (2 * kFieldBits));
+      if (g) atomicAdd(&ev_row[T.count_base + rep], g);
+      if (rs_row && (v >> 48)) atomicAdd(&rs_row[T.count_base + rep], v >> 48);
     }
     __syncthreads();
   }
 }
 
-// Full E/I/R counts of the current planes (initial state), same reduction
-// with the state masks in place of the event masks.
-template <int WS>
-__global__ void __launch_bounds__(256)
+// Full E/I/R counts of the planes (initial state): one shared atomic per
+// set bit, E | I << 21 | R << 42 per replica.
+__global__ void __launch_bounds__(kThreads)
     k_packed_count(PackedLayout L, const PackedTask *__restrict__ tasks,
                    const uint32_t *__restrict__ sa, const uint32_t *__restrict__ sb,
                    unsigned long long *__restrict__ out) {
-  constexpr int RG = 32 / WS;
-  __shared__ unsigned long long s_ev[WS * 32];
-  __shared__ unsigned long long s_rs[WS * 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
-  const int rsub = lane / WS, wsub = lane % WS;
-  const int W = L.words;
+  __shared__ unsigned long long s_ev[128 * 32];
   for (int ti = blockIdx.x; ti < L.n_tasks; ti += gridDim.x) {
     const PackedTask T = tasks[ti];
-    for (int j = threadIdx.x; j < WS * 32; j += blockDim.x) s_ev[j] = s_rs[j] = 0;
+    const int wbase = T.slice * 128;
+    const int nw = min(128, L.words - wbase);
+    for (int j = threadIdx.x; j < 128 * 32; j += blockDim.x) s_ev[j] = 0;
     __syncthreads();
-    const int word = T.slice * WS + wsub;
-    const bool word_ok = word < W;
-    uint32_t cE[kPlanes], cI[kPlanes], cR[kPlanes], cZ[kPlanes];
-#pragma unroll
-    for (int k = 0; k < kPlanes; ++k) cE[k] = cI[k] = cR[k] = cZ[k] = 0;
-    int rows = 0;
-    for (int base = T.row_begin + warp * RG; base < T.row_end; base += nwarps * RG) {
-      const int row = base + rsub;
-      if (word_ok && row < T.row_end) {
-        const int64_t idx = (int64_t)row * W + word;
-        const uint32_t a = sa[idx], b = sb[idx];
-        vc_add(cE, ~a & b);
-        vc_add(cI, a & ~b);
-        vc_add(cR, a & b);
-      }
-      ++rows;
-      if (__any_sync(kFull, rows == (1 << kPlanes) - 1)) {
-        flush_events<WS>(cE, cI, cR, cZ, s_ev, s_rs, wsub, rsub);
-        rows = 0;
-      }
+    const int64_t items = (int64_t)(T.row_end - T.row_begin) * nw;
+    for (int64_t it = threadIdx.x; it < items; it += blockDim.x) {
+      const int row = T.row_begin + (int)(it / nw);
+      const int wl = (int)(it % nw);
+      const int word = wbase + wl;
+      const uint32_t vm = word_mask(L, word);
+      const int64_t idx = (int64_t)row * L.words + word;
+      const uint32_t a = sa[idx] & vm, b = sb[idx] & vm;
+      count_bits(s_ev, wl, ~a & b, 1ull);
+      count_bits(s_ev, wl, a & ~b, 1ull << kFieldBits);
+      count_bits(s_ev, wl, a & b, 1ull << (2 * kFieldBits));
     }
-    flush_events<WS>(cE, cI, cR, cZ, s_ev, s_rs, wsub, rsub);
     __syncthreads();
-    for (int j = threadIdx.x; j < WS * 32; j += blockDim.x) {
-      const int rep = (T.slice * WS + (j >> 5)) * 32 + (j & 31);
+    for (int j = threadIdx.x; j < nw * 32; j += blockDim.x) {
+      const int rep = wbase * 32 + j;
       if (rep < L.m && s_ev[j]) atomicAdd(&out[T.count_base + rep], s_ev[j]);
     }
     __syncthreads();
   }
 }
 
-// Bernoulli(p0) initial infection per (node, replica), stream 1, same
-// uniforms as the plain path.  Writes planes and the step-0 mask.
+// Bernoulli(p0) initial infection per (node, replica), stream 1, the plain
+// path's uniforms.  Writes planes and the step-0 mask.
 __global__ void __launch_bounds__(256)
     k_packed_init(PackedLayout L, uint32_t *__restrict__ sa, uint32_t *__restrict__ sb,
                   uint32_t *__restrict__ mask, float p0, StepConsts c) {
@@ -291,14 +346,14 @@ __global__ void __launch_bounds__(256)
        idx += (int64_t)gridDim.x * blockDim.x) {
     const int32_t row = (int32_t)(idx / L.words);
     const int32_t word = (int32_t)(idx % L.words);
-    const uint32_t vmask = word == L.words - 1 ? L.last_mask : kFull;
+    const uint32_t vmask = word_mask(L, word);
     uint32_t inf = 0;
-    if (p0 > 0.0f) {
+    if (p0 > 0.0f && vmask) {
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         uint32_t x[4];
-        philox4x32_10((uint32_t)row, kStepInit, (uint32_t)(word * 8 + q), kStreamInit,
-                      c.key0, c.key1, x);
+        philox4x32_10((uint32_t)row, kStepInit, (uint32_t)(word * 8 + q), kStreamInit, c.key0,
+                      c.key1, x);
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc)
           if (unit24(x[cc]) < p0) inf |= 1u << (4 * q + cc);
@@ -326,8 +381,8 @@ __global__ void k_packed_pick(PackedLayout L, uint32_t *__restrict__ sa,
   const int32_t kk = k < n ? k : n;
   for (int32_t j = n - kk; j < n; ++j) {
     uint32_t x[4];
-    philox4x32_10((uint32_t)j, kStepPick, (uint32_t)r, kStreamPick + 4u * (uint32_t)net,
-                  c.key0, c.key1, x);
+    philox4x32_10((uint32_t)j, kStepPick, (uint32_t)r, kStreamPick + 4u * (uint32_t)net, c.key0,
+                  c.key1, x);
     const uint64_t r64 = (uint64_t)x[0] | ((uint64_t)x[1] << 32);
     const int32_t t = (int32_t)__umul64hi(r64, (uint64_t)(j + 1));
     const uint32_t old = atomicOr(&sa[(int64_t)(first + t) * L.words + word], bit);
@@ -388,57 +443,35 @@ __global__ void k_packed_classify(PackedLayout L, const uint32_t *__restrict__ s
   }
 }
 
-// Exposure only (test hook): exposure[i * m + r] exact int64.
+// Exposure only (test hook): exposure[i * m + r] exact int64, masks with
+// `W` words per node.
 __global__ void __launch_bounds__(256)
     k_packed_exposure(const int32_t *__restrict__ row_ptr, const int2 *__restrict__ ent,
                       int32_t n, const uint32_t *__restrict__ masks, int32_t W, int32_t m,
                       int64_t *__restrict__ exposure) {
-  const int64_t total = (int64_t)n * W;
+  const int64_t total = (int64_t)n * m;
   for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total;
        g += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t i = (int32_t)(g / W), w = (int32_t)(g % W);
-    int64_t acc[32];
-#pragma unroll
-    for (int r = 0; r < 32; ++r) acc[r] = 0;
+    const int32_t i = (int32_t)(g / m), r = (int32_t)(g % m);
+    int64_t acc = 0;
     for (int32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
       const int2 en = ent[k];
-      const uint32_t mm = masks[(int64_t)en.x * W + w];
-#pragma unroll
-      for (int r = 0; r < 32; ++r) acc[r] += ((mm >> r) & 1u) ? (int64_t)en.y : 0;
+      if ((masks[(int64_t)en.x * W + (r >> 5)] >> (r & 31)) & 1u) acc += en.y;
     }
-#pragma unroll
-    for (int r = 0; r < 32; ++r)
-      if (w * 32 + r < m) exposure[(int64_t)i * m + w * 32 + r] = acc[r];
+    exposure[g] = acc;
   }
 }
 
-template <int WS>
-void launch_step_ws(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
-                    const int2 *entries, const uint32_t *mask_in, uint32_t *mask_out,
-                    uint32_t *sa, uint32_t *sb, unsigned long long *ev_row,
-                    unsigned long long *rs_row, uint32_t step, float scale, bool wide,
-                    const StepConsts &c, int grid, cudaStream_t st) {
-  if (wide)
-    k_packed_step<WS, long long><<<grid, 256, 0, st>>>(L, tasks, row_ptr, entries, mask_in,
-                                                       mask_out, sa, sb, ev_row, rs_row, step,
-                                                       scale, c);
-  else
-    k_packed_step<WS, int><<<grid, 256, 0, st>>>(L, tasks, row_ptr, entries, mask_in, mask_out,
-                                                 sa, sb, ev_row, rs_row, step, scale, c);
-}
-
-int task_grid(int n_tasks) {
-  int g = n_tasks < 148 * 2 ? n_tasks : 148 * 2;
+int task_grid(int n_tasks, int per_sm) {
+  int g = n_tasks < 148 * per_sm ? n_tasks : 148 * per_sm;
   return g < 1 ? 1 : g;
 }
 
 }  // namespace
 
 void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb, uint32_t *mask, float p0,
-                 int32_t k_exact, const int32_t *net_of_row, const int32_t *net_first_row,
-                 const int32_t *net_rows, int32_t n_nets, const StepConsts &c,
-                 cudaStream_t st) {
-  (void)net_of_row;
+                 int32_t k_exact, const int32_t *net_first_row, const int32_t *net_rows,
+                 int32_t n_nets, const StepConsts &c, cudaStream_t st) {
   const int64_t total = (int64_t)L.n_nodes * L.words;
   k_packed_init<<<1184, 256, 0, st>>>(L, sa, sb, mask, k_exact > 0 ? 0.0f : p0, c);
   if (k_exact > 0) {
@@ -450,32 +483,22 @@ void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb, uint32_t *ma
 }
 
 void packed_step(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
-                 const int2 *entries, const uint32_t *mask_in, uint32_t *mask_out,
-                 uint32_t *sa, uint32_t *sb, unsigned long long *ev_row,
-                 unsigned long long *rs_row, uint32_t step, float scale, bool wide_acc,
-                 const StepConsts &c, cudaStream_t st) {
-  const int grid = task_grid(L.n_tasks);
-  switch (L.ws) {
-    case 1: launch_step_ws<1>(L, tasks, row_ptr, entries, mask_in, mask_out, sa, sb, ev_row, rs_row, step, scale, wide_acc, c, grid, st); break;
-    case 2: launch_step_ws<2>(L, tasks, row_ptr, entries, mask_in, mask_out, sa, sb, ev_row, rs_row, step, scale, wide_acc, c, grid, st); break;
-    case 4: launch_step_ws<4>(L, tasks, row_ptr, entries, mask_in, mask_out, sa, sb, ev_row, rs_row, step, scale, wide_acc, c, grid, st); break;
-    case 8: launch_step_ws<8>(L, tasks, row_ptr, entries, mask_in, mask_out, sa, sb, ev_row, rs_row, step, scale, wide_acc, c, grid, st); break;
-    case 16: launch_step_ws<16>(L, tasks, row_ptr, entries, mask_in, mask_out, sa, sb, ev_row, rs_row, step, scale, wide_acc, c, grid, st); break;
-    default: launch_step_ws<32>(L, tasks, row_ptr, entries, mask_in, mask_out, sa, sb, ev_row, rs_row, step, scale, wide_acc, c, grid, st); break;
-  }
+                 const int2 *entries, const uint32_t *mask_in, uint32_t *mask_out, uint32_t *sa,
+                 uint32_t *sb, uint32_t *evs, unsigned long long *ev_row,
+                 unsigned long long *rs_row, uint32_t step, float scale, const StepConsts &c,
+                 cudaStream_t st) {
+  k_infect<<<task_grid(L.n_tasks, 4), kThreads, 0, st>>>(
+      L, tasks, row_ptr, entries, reinterpret_cast<const uint4 *>(mask_in),
+      reinterpret_cast<const uint4 *>(sa), reinterpret_cast<const uint4 *>(sb),
+      reinterpret_cast<uint4 *>(evs), step, scale, c);
+  k_flow<<<task_grid(L.n_tasks, 4), kThreads, 0, st>>>(
+      L, tasks, row_ptr, reinterpret_cast<const uint4 *>(evs), reinterpret_cast<uint4 *>(mask_out),
+      reinterpret_cast<uint4 *>(sa), reinterpret_cast<uint4 *>(sb), ev_row, rs_row, step, c);
 }
 
 void packed_count(const PackedLayout &L, const PackedTask *tasks, const uint32_t *sa,
                   const uint32_t *sb, unsigned long long *counts_row, cudaStream_t st) {
-  const int grid = task_grid(L.n_tasks);
-  switch (L.ws) {
-    case 1: k_packed_count<1><<<grid, 256, 0, st>>>(L, tasks, sa, sb, counts_row); break;
-    case 2: k_packed_count<2><<<grid, 256, 0, st>>>(L, tasks, sa, sb, counts_row); break;
-    case 4: k_packed_count<4><<<grid, 256, 0, st>>>(L, tasks, sa, sb, counts_row); break;
-    case 8: k_packed_count<8><<<grid, 256, 0, st>>>(L, tasks, sa, sb, counts_row); break;
-    case 16: k_packed_count<16><<<grid, 256, 0, st>>>(L, tasks, sa, sb, counts_row); break;
-    default: k_packed_count<32><<<grid, 256, 0, st>>>(L, tasks, sa, sb, counts_row); break;
-  }
+  k_packed_count<<<task_grid(L.n_tasks, 2), kThreads, 0, st>>>(L, tasks, sa, sb, counts_row);
 }
 
 void packed_finalize_events(const unsigned long long *init, const unsigned long long *ev,

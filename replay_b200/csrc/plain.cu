@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256)
       any_s |= v[c4] == 0;
     }
     uint32_t x[4] = {0, 0, 0, 0};
-    if (any_s) philox4x32_10((uint32_t)i, step, (uint32_t)q, kStreamStep, c.key0, c.key1, x);
+    if (any_s) philox4x32_10((uint32_t)i, step, (uint32_t)q, kStreamInfect, c.key0, c.key1, x);
 #pragma unroll
     for (int c4 = 0; c4 < 4; ++c4) {
       const int32_t r = 4 * q + c4;
@@ -151,9 +151,10 @@ __device__ __forceinline__ float infection_x(const StepConsts &c, int32_t r, int
   return __fmul_rn(bs, ef);
 }
 
-// Geometric mode: S->E with P = 1 - exp(-beta_r * s_i * exposure), E->I,
-// I->R (or I->S), R->S with fixed per-step probabilities; one uniform per
-// (replica, node, step), event iff u < p.
+// Geometric mode: S->E with P = 1 - exp(-beta_r * s_i * exposure) against
+// the replica's infection uniform; E->I, I->R (or I->S), R->S with fixed
+// per-step probabilities against its bit-sliced flow uniform (flow_events on
+// this quad's bits of the replica word).
 __global__ void __launch_bounds__(256)
     k_transition_geometric(uint8_t *__restrict__ st, const int64_t *__restrict__ expo,
                            int32_t n, int32_t m, uint32_t step, float scale,
@@ -164,7 +165,8 @@ __global__ void __launch_bounds__(256)
   if (i < n) {
     uint8_t v[4];
     int64_t e[4];
-    bool need = false;
+    uint32_t Em = 0, Im = 0, Rm = 0;
+    bool any_exposed = false;
 #pragma unroll
     for (int c4 = 0; c4 < 4; ++c4) {
       const int32_t r = 4 * q + c4;
@@ -174,29 +176,37 @@ __global__ void __launch_bounds__(256)
         const int64_t idx = i + (int64_t)r * n;
         v[c4] = st[idx];
         if (v[c4] == 0) e[c4] = expo[idx];
-        need |= (v[c4] == 0 && e[c4] > 0) || v[c4] == 1 || v[c4] == 2 ||
-                (v[c4] == 3 && c.p_rs > 0.0f);
+        any_exposed |= v[c4] == 0 && e[c4] > 0;
+        const uint32_t bit = 1u << (r & 31);
+        Em |= v[c4] == 1 ? bit : 0u;
+        Im |= v[c4] == 2 ? bit : 0u;
+        Rm |= v[c4] == 3 ? bit : 0u;
       }
     }
     uint32_t x[4] = {0, 0, 0, 0};
-    if (need) philox4x32_10((uint32_t)i, step, (uint32_t)q, kStreamStep, c.key0, c.key1, x);
+    if (any_exposed)
+      philox4x32_10((uint32_t)i, step, (uint32_t)q, kStreamInfect, c.key0, c.key1, x);
+    const uint32_t ev = (Em | Im | Rm)
+                            ? flow_events(Em, Im, Rm, c.th, c.key0, c.key1, (uint32_t)i, step,
+                                          (uint32_t)(q >> 3))
+                            : 0u;
 #pragma unroll
     for (int c4 = 0; c4 < 4; ++c4) {
       const int32_t r = 4 * q + c4;
       if (r >= m) continue;
       uint8_t nv = v[c4];
-      const float u = unit24(x[c4]);
+      const bool fired = (ev >> (r & 31)) & 1u;
       if (v[c4] == 0) {
         if (e[c4] > 0) {
           const float P = one_minus_exp_neg(infection_x(c, r, i, e[c4], scale));
-          if (P > u) nv = c.has_exposed ? 1 : 2;
+          if (P > unit24(x[c4])) nv = c.has_exposed ? 1 : 2;
         }
       } else if (v[c4] == 1) {
-        if (u < c.p_ei) nv = 2;
+        if (fired) nv = 2;
       } else if (v[c4] == 2) {
-        if (u < c.p_ir) nv = c.ir_to_s ? 0 : 3;
+        if (fired) nv = c.ir_to_s ? 0 : 3;
       } else {
-        if (c.p_rs > 0.0f && u < c.p_rs) nv = 0;
+        if (fired) nv = 0;
       }
       if (nv != v[c4]) st[i + (int64_t)r * n] = nv;
       cls[c4] = nv;

@@ -3,6 +3,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "rp_internal.h"
+
 namespace rp {
 
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): 10 rounds of two
@@ -40,14 +42,20 @@ __device__ __forceinline__ float unit24(uint32_t x) {
   return __fmul_rn(__uint2float_rn((x >> 8) + 1u), 0x1p-24f);
 }
 
-// Random stream layout: key = seed; counter = (node, step, replica / 4,
-// stream); output word replica % 4.  Stream 0 drives the per-step
-// transitions, stream 1 the Bernoulli initial condition (step 0xFFFFFFFF),
-// stream 2 the exact-count initial condition (node = draw index,
-// step 0xFFFFFFFE, third word = replica).
-constexpr uint32_t kStreamStep = 0u;
+// Random stream layout, key = seed, counter = (node, step, c2, c3):
+//  * infection (S->E / S->I) uniform of replica r: c2 = r / 4, c3 = 3,
+//    output r % 4 on the 24-bit grid; event iff P > u;
+//  * flow (E->I, I->R, R->S) uniform of replica r: bit-sliced -- bit k of
+//    U_r (k = 0 is 2^-1) is bit r % 32 of output k % 4 of counter
+//    (node, step, r / 32, (k / 4) << 4); event iff U_r < floor(p 2^64)
+//    over the first 64 bits (flow_events);
+//  * Bernoulli initial condition: step 0xFFFFFFFF, c2 = r / 4, c3 = 1;
+//  * exact-count initial condition (Floyd): node = draw j, step
+//    0xFFFFFFFE, c2 = r, c3 = 2 (+ 4 x network index).
+constexpr uint32_t kStreamFlow = 0u;    // bit-sliced flow uniforms, c3 = plane/4 << 4
 constexpr uint32_t kStreamInit = 1u;
 constexpr uint32_t kStreamPick = 2u;
+constexpr uint32_t kStreamInfect = 3u;  // scalar infection uniforms
 constexpr uint32_t kStepInit = 0xFFFFFFFFu;
 constexpr uint32_t kStepPick = 0xFFFFFFFEu;
 
@@ -81,6 +89,42 @@ __device__ __forceinline__ float one_minus_exp_neg(float x) {
   const float scale = __int_as_float((127 - k) << 23);
   const float e = __fmul_rn(__fadd_rn(1.0f, em1), scale);
   return __fsub_rn(1.0f, e);
+}
+
+// Per-step flow thresholds (FlowThresholds, rp_internal.h) hold
+// floor(p 2^64); p >= 1 is a certain event, p <= 0 none.
+// Flow events of the replicas selected by E, I, R (disjoint masks of one
+// 32-replica word of `node`): replica r moves iff its bit-sliced uniform is
+// below its state's threshold.  All 32 replicas are compared at once, one
+// random plane per bit, stopping when every candidate is decided (about
+// log2(candidates) + 2 planes).  Returns the event mask.
+__device__ __forceinline__ uint32_t flow_events(uint32_t E, uint32_t I, uint32_t R,
+                                                const FlowThresholds &th, uint32_t key0,
+                                                uint32_t key1, uint32_t node, uint32_t step,
+                                                uint32_t word) {
+  uint32_t lt = (th.te_all ? E : 0u) | (th.ti_all ? I : 0u) | (th.tr_all ? R : 0u);
+  const uint32_t e2 = (th.te_all || th.te == 0) ? 0u : E;
+  const uint32_t i2 = (th.ti_all || th.ti == 0) ? 0u : I;
+  const uint32_t r2 = (th.tr_all || th.tr == 0) ? 0u : R;
+  uint32_t und = e2 | i2 | r2;
+  for (int j = 0; und != 0u && j < 16; ++j) {
+    uint32_t x[4];
+    philox4x32_10(node, step, word, (uint32_t)j << 4, key0, key1, x);
+    const int sh = 60 - 4 * j;
+    const uint32_t ce = (uint32_t)(th.te >> sh) & 0xFu;
+    const uint32_t ci = (uint32_t)(th.ti >> sh) & 0xFu;
+    const uint32_t cr = (uint32_t)(th.tr >> sh) & 0xFu;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t b = 3 - q;
+      const uint32_t T = (((ce >> b) & 1u) ? e2 : 0u) | (((ci >> b) & 1u) ? i2 : 0u) |
+                         (((cr >> b) & 1u) ? r2 : 0u);
+      const uint32_t w = x[q];
+      lt |= und & T & ~w;
+      und &= ~(T ^ w);
+    }
+  }
+  return lt;
 }
 
 // Countdown arithmetic of the reference (int op float, truncated back to

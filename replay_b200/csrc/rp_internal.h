@@ -10,6 +10,11 @@
 
 namespace rp {
 
+struct FlowThresholds {
+  unsigned long long te, ti, tr;
+  int te_all, ti_all, tr_all;
+};
+
 // ---- errors ---------------------------------------------------------------
 void set_error(const char *fmt, ...);
 rp_status cuda_fail(cudaError_t e, const char *what);
@@ -154,6 +159,7 @@ void enqueue_window_compact(WindowWorkspace &ws, int32_t *row_ptr_out,
 // ---- kernels of the step loop -------------------------------------------------
 struct StepConsts {
   uint32_t key0, key1;
+  FlowThresholds th;  // p_ei, p_ir, p_rs as 64-bit fixed point
   float step_size;
   float neg_log_base;  // -logf(1 - infect_prob), countdown mode
   int32_t upper, medium, lower, E, I, R;  // countdown ranges / durations
@@ -183,27 +189,29 @@ void plain_classify(int transition, const void *state, int32_t n, int32_t m,
 // Batched path (bit-packed replica words).
 struct PackedTask {
   int32_t row_begin, row_end;  // rows of one network
-  int32_t slice;               // 32-word slice (or the only slice)
+  int32_t slice;               // 32 four-word columns (128 words) per slice
   int32_t count_base;          // index of replica 0 of this network in counts
 };
 struct PackedLayout {
-  int32_t n_nodes, words, m;  // m: replicas per network
-  int32_t ws;                 // words per row group (1..32, power of 2)
-  uint32_t last_mask;         // valid bits of the last word
+  int32_t n_nodes;
+  int32_t words;      // words per node row, padded to a multiple of 4
+  int32_t vwords;     // words holding replicas: ceil(m / 32)
+  int32_t q4;         // four-word columns per row (words / 4)
+  int32_t m;          // replicas per network
+  uint32_t last_mask; // valid bits of word vwords - 1
+  int32_t lpr;        // lanes per row (power of 2, <= 32)
   int32_t n_tasks;
-  int32_t counts_stride;      // u64 entries per count row
 };
 void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb,
                  uint32_t *mask, float p0, int32_t k_exact,
-                 const int32_t *net_of_row, const int32_t *net_first_row,
-                 const int32_t *net_rows, int32_t n_nets,
-                 const StepConsts &c, cudaStream_t st);
+                 const int32_t *net_first_row, const int32_t *net_rows,
+                 int32_t n_nets, const StepConsts &c, cudaStream_t st);
 void packed_step(const PackedLayout &L, const PackedTask *tasks,
                  const int32_t *row_ptr, const int2 *entries,
                  const uint32_t *mask_in, uint32_t *mask_out, uint32_t *sa,
-                 uint32_t *sb, unsigned long long *ev_row,
+                 uint32_t *sb, uint32_t *evs, unsigned long long *ev_row,
                  unsigned long long *rs_row, uint32_t step, float scale,
-                 bool wide_acc, const StepConsts &c, cudaStream_t st);
+                 const StepConsts &c, cudaStream_t st);
 void packed_count(const PackedLayout &L, const PackedTask *tasks,
                   const uint32_t *sa, const uint32_t *sb,
                   unsigned long long *counts_row, cudaStream_t st);

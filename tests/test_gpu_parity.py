@@ -124,6 +124,7 @@ GEOMETRIC_CASES = [
     dict(M=64, iterations=40, beta=6e-4, p_ei=0.3, p_ir=0.2, p_rs=0.1, initial_count=4),
     dict(M=40, iterations=30, beta=5e-4, p_ir=0.2, has_exposed=False, ir_to_s=True, initial_count=5),
     dict(M=96, iterations=24, beta=3e-4, p_ei=0.25, p_ir=0.1, initial_count=2, window=7200),
+    dict(M=45, iterations=20, beta=1e-3, p_ei=1.0, p_ir=3e-9, p_rs=0.5, initial_count=6),
 ]
 
 
