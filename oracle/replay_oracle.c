@@ -110,6 +110,36 @@ int orc_flow_event(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica
   return 0;
 }
 
+/* Bit-sliced comparison U_r < T over 64 bits: bit k of U_r (k = 0 is 2^-1)
+ * is bit (r % 32) of output k % 4 of Philox(key = seed, counter = (node,
+ * step, r / 32, tag | (k / 4) << 4)). */
+static int sliced_less(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica,
+                       uint32_t tag, uint64_t T) {
+  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  const uint32_t bit = replica & 31u;
+  for (int j = 0; j < 16; j++) {
+    uint32_t ctr[4] = {node, step, replica >> 5, tag | ((uint32_t)j << 4)};
+    uint32_t x[4];
+    orc_philox4x32_10(ctr, key, x);
+    for (int q = 0; q < 4; q++) {
+      const int k = 4 * j + q;
+      const uint32_t wb = (x[q] >> bit) & 1u;
+      const uint32_t tb = (uint32_t)(T >> (63 - k)) & 1u;
+      if (wb != tb) return wb < tb;
+    }
+  }
+  return 0;
+}
+
+/* Infection decision of replica r (geometric mode): its per-step uniform is
+ * bit-sliced on tag 4; event iff U_r < floor(P 2^64); P >= 1 always
+ * infects, P <= 0 (or NaN) never. */
+int orc_infect_event(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica, float P) {
+  if (!(P > 0.0f)) return 0;
+  if (P >= 1.0f) return 1;
+  return sliced_less(seed, node, step, replica, 4u, (uint64_t)ldexp((double)P, 64));
+}
+
 /* 1 - exp(-x) for x >= 0 using only correctly rounded +,-,*: Cody-Waite
  * reduction x = k ln2 + r, |r| <= ln2/2, and the Taylor series of expm1(-r)
  * through r^9/9!.  The device code performs the identical sequence with
@@ -869,8 +899,8 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
               float ef = (float)expi[idx];
               if (scale[t] != 1.0f) ef = ef * scale[t];
               float P = orc_one_minus_exp_neg(bs * ef);
-              float uu = orc_uniform(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, 3u);
-              if (P > uu) cd[idx] = p->has_exposed ? 1 : 2;
+              if (orc_infect_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, P))
+                cd[idx] = p->has_exposed ? 1 : 2;
             }
           } else if (st == 1) {
             if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, te, te_all))

@@ -22,8 +22,10 @@ extern "C" {
 
 /* ---- counter-based random numbers ---------------------------------------- *
  * key = seed; counter = (node, step, c2, c3):
- *   infection (S->E, S->I) uniform of replica r: c2 = r / 4, c3 = 3, output
+ *   countdown infection uniform of replica r: c2 = r / 4, c3 = 3, output
  *     r % 4, as the 24-bit grid value ((x >> 8) + 1) 2^-24; event iff P > u;
+ *   geometric infection uniform: bit-sliced on tag 4 (orc_infect_event),
+ *     event iff U < floor(P 2^64);
  *   flow (E->I, I->R, R->S) uniform of replica r: bit-sliced, see
  *     orc_flow_event;
  *   initial Bernoulli: step = 0xFFFFFFFF, c2 = r / 4, c3 = 1;
@@ -36,6 +38,7 @@ float orc_uniform(uint64_t seed, uint32_t node, uint32_t step,
                   uint32_t replica, uint32_t stream);
 float orc_one_minus_exp_neg(float x);
 uint64_t orc_threshold64(float p, int *always);
+int orc_infect_event(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica, float P);
 int orc_flow_event(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica,
                    uint64_t T, int always);
 

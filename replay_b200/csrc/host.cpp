@@ -129,7 +129,7 @@ struct rp_sim {
   // plain state
   DevBuf state, exposure;
   // batched state
-  DevBuf sa, sb, mask[2], evs, tasks, ev, rs, init_counts;
+  DevBuf sa, sb, mask, evs, flag, tasks, ev, rs, init_counts;
   PackedLayout L{};
   DevBuf net_size, net_first, net_rows;
   int32_t n_nets = 1;
@@ -209,8 +209,8 @@ struct rp_sim {
       RP_TRY_CUDA(cudaMemsetAsync(ev.ptr, 0, ev.bytes, st));
       if (rs.ptr && p.p_rs > 0.0f) RP_TRY_CUDA(cudaMemsetAsync(rs.ptr, 0, rs.bytes, st));
       RP_TRY_CUDA(cudaMemsetAsync(init_counts.ptr, 0, init_counts.bytes, st));
-      packed_init(L, sa.as<uint32_t>(), sb.as<uint32_t>(), mask[0].as<uint32_t>(),
-                  p.initial_infected, p.initial_count, net_first.as<int32_t>(),
+      packed_init(L, sa.as<uint32_t>(), sb.as<uint32_t>(), mask.as<uint32_t>(),
+                  flag.as<uint8_t>(), p.initial_infected, p.initial_count, net_first.as<int32_t>(),
                   net_rows.as<int32_t>(), n_nets, c, st);
       packed_count(L, tasks.as<PackedTask>(), sa.as<uint32_t>(), sb.as<uint32_t>(),
                    init_counts.as<unsigned long long>(), st);
@@ -236,13 +236,16 @@ struct rp_sim {
         mark(kMarkStep);
         k += 2;
       } else {
-        packed_step(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t),
-                    mask[t & 1].as<uint32_t>(), mask[(t + 1) & 1].as<uint32_t>(),
-                    sa.as<uint32_t>(), sb.as<uint32_t>(), evs.as<uint32_t>(),
+        packed_infect(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t), mask.as<uint32_t>(),
+                      sa.as<uint32_t>(), sb.as<uint32_t>(), evs.as<uint32_t>(),
+                      flag.as<uint8_t>(), (uint32_t)t, step_scale[t], c, st);
+        mark(kMarkSpmv);
+        packed_flow(L, tasks.as<PackedTask>(), rp_of(t), mask.as<uint32_t>(), sa.as<uint32_t>(),
+                    sb.as<uint32_t>(), evs.as<uint32_t>(), flag.as<uint8_t>(),
                     ev.as<unsigned long long>() + (int64_t)t * per_row,
                     p.p_rs > 0.0f ? rs.as<unsigned long long>() + (int64_t)t * per_row
                                   : nullptr,
-                    (uint32_t)t, step_scale[t], c, st);
+                    (uint32_t)t, c, st);
         mark(kMarkStep);
         k += 2;
       }
@@ -373,6 +376,10 @@ rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
   // ---- constants ----
   s.c.key0 = (uint32_t)p.seed;
   s.c.key1 = (uint32_t)(p.seed >> 32);
+  for (int r = 0; r < 10; ++r) {
+    s.c.rk[2 * r] = s.c.key0 + (uint32_t)r * 0x9E3779B9u;
+    s.c.rk[2 * r + 1] = s.c.key1 + (uint32_t)r * 0xBB67AE85u;
+  }
   s.c.step_size = p.step_size;
   s.c.neg_log_base = -logf(1.0f - p.infect_prob);
   s.c.E = p.exposed_duration;
@@ -410,15 +417,13 @@ rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
   return RP_OK;
 }
 
-// Rows per batched task, by graph size: enough tasks for every SM to hold
-// two CTAs, each task long enough to amortise its count flush.
-int32_t rows_per_task(int32_t n_rows, int32_t n_slices, int32_t rg) {
-  const int64_t target_tasks = 148 * 2 * 4;
+// Rows per batched task: about one wave of CTAs (148 SMs x 3), at most 1024
+// rows (the kernels stage a task's row pointers in shared memory).
+int32_t rows_per_task(int32_t n_rows, int32_t n_slices) {
+  const int64_t target_tasks = 148 * 3;
   int64_t rows = ((int64_t)n_rows * n_slices + target_tasks - 1) / target_tasks;
-  const int64_t quantum = 8 * rg;
-  if (rows < quantum) rows = quantum;
-  if (rows > 8192) rows = 8192;
-  rows = (rows + quantum - 1) / quantum * quantum;
+  if (rows < 32) rows = 32;
+  if (rows > 1024) rows = 1024;
   return (int32_t)rows;
 }
 
@@ -446,7 +451,6 @@ rp_status alloc_state(rp_sim &s) {
   while (lpr < L.q4 && lpr < 32) lpr <<= 1;
   L.lpr = lpr;
   const int32_t n_slices = (L.q4 + 31) / 32;
-  const int32_t rg = 32 / lpr;
   std::vector<PackedTask> tasks;
   std::vector<int32_t> first, rows, size;
   // single network: rows [0, N)
@@ -454,19 +458,20 @@ rp_status alloc_state(rp_sim &s) {
   rows.push_back(N);
   size.push_back(N);
   for (int net = 0; net < s.n_nets; ++net) {
-    const int32_t rpt = rows_per_task(rows[net], n_slices, rg);
+    const int32_t rpt = rows_per_task(rows[net], n_slices);
     for (int32_t r0 = first[net]; r0 < first[net] + rows[net]; r0 += rpt)
       for (int32_t sl = 0; sl < n_slices; ++sl)
         tasks.push_back(PackedTask{r0, std::min(r0 + rpt, first[net] + rows[net]), sl,
                                    net * M});
   }
   L.n_tasks = (int32_t)tasks.size();
+  RP_TRY(packed_prepare());
   const size_t plane = sizeof(uint32_t) * (size_t)N * L.words;
   RP_TRY(s.sa.alloc(plane));
   RP_TRY(s.sb.alloc(plane));
-  RP_TRY(s.mask[0].alloc(plane));
-  RP_TRY(s.mask[1].alloc(plane));
+  RP_TRY(s.mask.alloc(plane));
   RP_TRY(s.evs.alloc(plane));
+  RP_TRY(s.flag.alloc(((size_t)N * L.q4 + 3) / 4 * 4));
   RP_TRY(s.tasks.alloc(sizeof(PackedTask) * tasks.size()));
   RP_TRY_CUDA(cudaMemcpy(s.tasks.ptr, tasks.data(), sizeof(PackedTask) * tasks.size(),
                          cudaMemcpyHostToDevice));
@@ -757,7 +762,7 @@ RP_API rp_status rp_sim_get_info(const rp_sim *s, rp_sim_info *o) {
   o->prebuilt_nnz = s->prebuilt_nnz;
   int64_t bytes = 0;
   const DevBuf *bufs[] = {&s->arena_rp, &s->arena_ent, &s->state, &s->exposure, &s->sa,
-                          &s->sb, &s->mask[0], &s->mask[1], &s->evs, &s->tasks, &s->ev, &s->rs,
+                          &s->sb, &s->mask, &s->evs, &s->flag, &s->tasks, &s->ev, &s->rs,
                           &s->init_counts, &s->counts, &s->beta_r, &s->sus, &s->classes,
                           &s->wsp.hits, &s->wsp.entries, &s->wsp.erank, &s->wsp.tmp_e,
                           &s->wsp.tmp_r, &s->wsp.row_ptr, &s->wsp.deg, &s->wsp.tiles,
@@ -814,7 +819,7 @@ RP_API rp_status rp_sim_profile_steps(rp_sim *s, float *step_ms) {
     RP_TRY_CUDA(cudaEventElapsedTime(&ms, mk.ev[i - 1], mk.ev[i]));
     if (mk.kind[i] == rp_sim::kMarkSpmv && t < s->T) step_ms[t] = ms;
     if (mk.kind[i] == rp_sim::kMarkStep && t < s->T) {
-      step_ms[t] = (s->path == RP_PATH_PLAIN ? step_ms[t] : 0.0f) + ms;
+      step_ms[t] += ms;
       ++t;
     }
   }

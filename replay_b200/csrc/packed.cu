@@ -5,20 +5,23 @@
 // 16-byte access:
 //   sa, sb    state planes; replica bit (a, b): S (0,0), E (0,1), I (1,0),
 //             R (1,1)
-//   mask_t    infectious bits of step t (a & ~b), double-buffered: step t
-//             reads mask_t and writes mask_{t+1}
-//   evs       infection events of the step, written for rows with contacts
+//   mask      infectious bits (a & ~b); k_infect reads it, then k_flow
+//             rewrites the words whose state changed
+//   evs       infection events of the step (items with events only; a
+//             per-item flag byte tells k_flow which ones)
 // The window CSR holds {col, weight} pairs (int32 contact-seconds).
 //
 // k_infect (exposure SpMM + infection draws), per row with contacts, lanes
 // over 4-word columns (the replacement of cusparseSpMM,
 // tool/gpu_cpu_temporal_sim.cu:1062, and monte_carlo_simulation, :137-159):
 //   1. inf = OR over neighbours j of mask_t[j] (16 B per lane per entry);
-//   2. exposed = inf & S; the quads (4 replicas) holding exposed replicas are
-//      compacted across the warp so every lane draws: exact int64 exposure
-//      sums of the quad's replicas over the row's entries, one Philox call,
-//      P = 1 - exp(-beta_r s_i e) > u (the replica's infection uniform);
-//   3. events go to evs.
+//   2. exposed = inf & S; the exposed replicas of a word compare their
+//      bit-sliced infection uniforms with the word bound B = max bs_r *
+//      e_max (e_max = the row's total contact-seconds, so every P <= B), 32
+//      replicas per random plane; only replicas below B compute their exact
+//      int64 exposure and P = 1 - exp(-beta_r s_i e) and finish the
+//      comparison against floor(P 2^64) (infect_event);
+//   3. events go to evs and the item's flag.
 // k_flow (transitions + count reduction), every (row, 4-word column):
 //   reads the planes and the row's infection events, draws the bit-sliced
 //   flow uniforms of the E, I (and waning R) replicas, 32 replicas per random
@@ -58,144 +61,270 @@ __device__ __forceinline__ uint32_t nibble_any(uint32_t x) {
   return o;
 }
 
+__device__ __forceinline__ void or4(uint4 &a, const uint4 b) {
+  a.x |= b.x;
+  a.y |= b.y;
+  a.z |= b.z;
+  a.w |= b.w;
+}
+
+// Fast division of an item index by the columns of a task (ncols <= 32,
+// items < 2^27): q = umulhi(i, ceil(2^32 / d)).
+struct Div {
+  uint32_t d, mag;
+  __device__ explicit Div(uint32_t dd) : d(dd), mag(dd > 1 ? 0xFFFFFFFFu / dd + 1u : 0u) {}
+  __device__ uint32_t div(uint32_t i) const { return d > 1 ? __umulhi(i, mag) : i; }
+};
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int &total) {
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  total = __shfl_sync(kFull, incl, 31);
+  return incl - v;
+}
+
+__device__ __forceinline__ int find_owner(const int32_t *off, int p) {
+  int owner = 0;
+#pragma unroll
+  for (int st = 16; st > 0; st >>= 1)
+    if (off[owner + st] <= p) owner += st;
+  return owner;
+}
+
+constexpr int kMaxTaskRows = 1024;  // rows of one task (host-side limit)
+
+constexpr int kEntCap = 1024;       // staged CSR pairs per chunk
+
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads)
+// Per-warp scratch of k_infect (dynamic shared memory).
+struct InfectScratch {
+  int32_t off[32];        // warp scan offsets
+  uint32_t cnt4[32];      // per lane: words (phase 2) or candidate bits (phase 3)
+  int32_t rloc[32];       // task-relative row of each lane's item
+  int32_t col[32];        // column of each lane's item
+  float efmax[32];        // ef(e_max) of the item's row
+  uint32_t X[32][4];      // exposed replicas per word
+  uint32_t C[32][4];      // candidates per word (after the bound test)
+  uint32_t pl[32][4][4];  // first 4 random planes of each word
+  uint8_t have[32][4];    // planes kept (0 or 4)
+  uint32_t ev[32][4];     // infection events
+};
+
+constexpr int kInfectDynSmem = kEntCap * 8 + 128 * 32 * 4 + kWarps * (int)sizeof(InfectScratch);
+
+// k-th set bit over a lane's four 32-bit masks (k >= 0, exists).
+__device__ __forceinline__ void kth_bit4(const uint32_t *m, int k, int &w, int &b) {
+  w = 0;
+  while (k >= __popc(m[w])) {
+    k -= __popc(m[w]);
+    ++w;
+  }
+  uint32_t t = m[w];
+  for (; k > 0; --k) t &= t - 1;
+  b = __ffs(t) - 1;
+}
+
+// One item (row, 4-word column) per lane; the item's global loads (the
+// neighbours' mask words and its planes) are issued together.  Exposed words
+// are then compacted across the warp for the bound test (phase 2), and the
+// surviving candidate replicas compacted again for the exact test (phase 3),
+// so that every lane works on a dense list.
+__global__ void __launch_bounds__(kThreads, 3)
     k_infect(PackedLayout L, const PackedTask *__restrict__ tasks,
              const int32_t *__restrict__ row_ptr, const int2 *__restrict__ ent,
              const uint4 *__restrict__ mask_in, const uint4 *__restrict__ sa,
-             const uint4 *__restrict__ sb, uint4 *__restrict__ evs, uint32_t step, float scale,
-             StepConsts c) {
-  __shared__ uint32_t s_exp[kWarps][32][4];
-  __shared__ uint32_t s_ev[kWarps][32][4];
-  __shared__ int32_t s_off[kWarps][32];
-  __shared__ uint32_t s_qm[kWarps][32];
-  __shared__ int32_t s_row[kWarps][32];
-  __shared__ int32_t s_col[kWarps][32];
+             const uint4 *__restrict__ sb, uint4 *__restrict__ evs,
+             uint32_t *__restrict__ flag32, uint32_t step, float scale, StepConsts c) {
+  __shared__ int32_t s_rp[kMaxTaskRows + 1];
+  __shared__ float s_bw[128];  // max |beta_r| of each word of the slice
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  int2 *s_ent = reinterpret_cast<int2 *>(s_dyn);
+  float *s_beta = reinterpret_cast<float *>(s_dyn + kEntCap * sizeof(int2));
+  InfectScratch &S = reinterpret_cast<InfectScratch *>(
+      s_dyn + kEntCap * sizeof(int2) + 128 * 32 * sizeof(float))[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int lpr = L.lpr, rpw = 32 / lpr;
-  const int rsub = lane / lpr, csub = lane % lpr;
   const uint32_t *mask_w = reinterpret_cast<const uint32_t *>(mask_in);
   for (int ti = blockIdx.x; ti < L.n_tasks; ti += gridDim.x) {
     const PackedTask T = tasks[ti];
     const int cbase = T.slice * 32;
     const int ncols = min(32, L.q4 - cbase);
-    for (int base = T.row_begin + warp * rpw; base < T.row_end; base += kWarps * rpw) {
-      const int row = base + rsub;
-      const bool row_ok = row < T.row_end;
-      int32_t beg = 0, end = 0;
-      if (row_ok) {
-        beg = row_ptr[row];
-        end = row_ptr[row + 1];
+    const Div dv((uint32_t)ncols);
+    const int nrows = T.row_end - T.row_begin;
+    for (int i = threadIdx.x; i <= nrows; i += blockDim.x) s_rp[i] = row_ptr[T.row_begin + i];
+    if (c.beta_r) {
+      for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x)
+        s_beta[j] = cbase * 128 + j < L.m ? c.beta_r[cbase * 128 + j] : 0.0f;
+      __syncthreads();
+      for (int wl = threadIdx.x; wl < ncols * 4; wl += blockDim.x) {
+        float mx = 0.0f;
+        for (int r = 0; r < 32; ++r) mx = fmaxf(mx, fabsf(s_beta[wl * 32 + r]));
+        s_bw[wl] = mx;
       }
-      const bool nonempty = row_ok && end > beg;
-      // ---- OR of the neighbours' infectious words, 4 columns per lane ----
-      // (warp-uniform trip count: the compaction below shuffles)
-      for (int cc0 = 0; cc0 < ncols; cc0 += lpr) {
-        const int cc = cc0 + csub;
-        const bool col_ok = cc < ncols;
-        const int col = cbase + (col_ok ? cc : 0);
-        uint4 inf = make_uint4(0, 0, 0, 0);
-        if (nonempty && col_ok) {
-          int32_t k = beg;
-          for (; k + 2 <= end; k += 2) {
-            const int2 e0 = ent[k], e1 = ent[k + 1];
-            const uint4 m0 = mask_in[(int64_t)e0.x * L.q4 + col];
-            const uint4 m1 = mask_in[(int64_t)e1.x * L.q4 + col];
-            inf.x |= m0.x | m1.x;
-            inf.y |= m0.y | m1.y;
-            inf.z |= m0.z | m1.z;
-            inf.w |= m0.w | m1.w;
-          }
-          if (k < end) {
-            const int2 e0 = ent[k];
-            const uint4 m0 = mask_in[(int64_t)e0.x * L.q4 + col];
-            inf.x |= m0.x;
-            inf.y |= m0.y;
-            inf.z |= m0.z;
-            inf.w |= m0.w;
-          }
-        }
-        uint32_t ex[4] = {0, 0, 0, 0};
-        if (inf.x | inf.y | inf.z | inf.w) {
+    }
+    __syncthreads();
+    for (int r0 = 0; r0 < nrows;) {
+      // chunk of rows whose CSR pairs fit the staging buffer (>= 1 row)
+      int lo = r0 + 1, hi = nrows;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_rp[mid] - s_rp[r0] <= kEntCap) lo = mid; else hi = mid - 1;
+      }
+      const int r1 = lo;
+      const int32_t e0 = s_rp[r0], e1 = s_rp[r1];
+      const bool staged = e1 - e0 <= kEntCap;
+      if (staged)
+        for (int k = threadIdx.x; k < e1 - e0; k += blockDim.x) s_ent[k] = ent[e0 + k];
+      __syncthreads();
+      const int nitems = (r1 - r0) * ncols;
+      for (int it0 = warp * 32; it0 < nitems; it0 += kWarps * 32) {  // warp-uniform
+        // ---- phase 1: gather, per lane ----
+        const int it = it0 + lane;
+        const bool ok = it < nitems;
+        const int rl = ok ? (int)dv.div((uint32_t)it) : 0;
+        const int cc = ok ? it - rl * ncols : 0;
+        const int rloc = r0 + rl;
+        const int col = cbase + cc;
+        const int row = T.row_begin + rloc;
+        const int32_t beg = s_rp[rloc], end = s_rp[rloc + 1];
+        const int n = ok ? end - beg : 0;
+        uint32_t X[4] = {0, 0, 0, 0};
+        float efmax = 0.0f;
+        if (n > 0) {
           const int64_t idx = (int64_t)row * L.q4 + col;
-          const uint4 a = sa[idx], b = sb[idx];
+          const uint4 a4 = sa[idx], b4 = sb[idx];
+          const int2 *er = staged ? s_ent + (beg - e0) : ent + beg;
+          uint4 inf = make_uint4(0, 0, 0, 0);
+          long long emax = 0;
+          int k = 0;
+          for (; k + 4 <= n; k += 4) {
+            const int2 q0 = er[k], q1 = er[k + 1], q2 = er[k + 2], q3 = er[k + 3];
+            const uint4 m0 = mask_in[(int64_t)q0.x * L.q4 + col];
+            const uint4 m1 = mask_in[(int64_t)q1.x * L.q4 + col];
+            const uint4 m2 = mask_in[(int64_t)q2.x * L.q4 + col];
+            const uint4 m3 = mask_in[(int64_t)q3.x * L.q4 + col];
+            or4(inf, m0);
+            or4(inf, m1);
+            or4(inf, m2);
+            or4(inf, m3);
+            emax += (long long)q0.y + q1.y + q2.y + q3.y;
+          }
+          for (; k < n; ++k) {
+            const int2 q0 = er[k];
+            or4(inf, mask_in[(int64_t)q0.x * L.q4 + col]);
+            emax += q0.y;
+          }
 #pragma unroll
           for (int w = 0; w < 4; ++w)
-            ex[w] = get4(inf, w) & ~get4(a, w) & ~get4(b, w) & word_mask(L, 4 * col + w);
+            X[w] = get4(inf, w) & ~get4(a4, w) & ~get4(b4, w) & word_mask(L, 4 * col + w);
+          efmax = __ll2float_rn(emax);
+          if (scale != 1.0f) efmax = __fmul_rn(efmax, scale);
         }
-        uint32_t qm = 0;
+        const uint32_t wm = (X[0] ? 1u : 0u) | (X[1] ? 2u : 0u) | (X[2] ? 4u : 0u) | (X[3] ? 8u : 0u);
+        if (!__any_sync(kFull, wm != 0)) continue;
+        int total;
+        S.off[lane] = warp_excl_scan(__popc(wm), lane, total);
+        S.cnt4[lane] = wm;
+        S.rloc[lane] = rloc;
+        S.col[lane] = col;
+        S.efmax[lane] = efmax;
 #pragma unroll
-        for (int w = 0; w < 4; ++w) qm |= nibble_any(ex[w]) << (8 * w);
-        // ---- compact the exposed quads of the warp ----
-        const int cnt = __popc(qm);
-        int incl = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int y = __shfl_up_sync(kFull, incl, o);
-          if (lane >= o) incl += y;
+        for (int w = 0; w < 4; ++w) {
+          S.X[lane][w] = X[w];
+          S.C[lane][w] = 0;
+          S.ev[lane][w] = 0;
         }
-        const int total = __shfl_sync(kFull, incl, 31);
-        if (total) {
-          s_off[warp][lane] = incl - cnt;
-          s_qm[warp][lane] = qm;
-          s_row[warp][lane] = row;
-          s_col[warp][lane] = col;
-#pragma unroll
-          for (int w = 0; w < 4; ++w) {
-            s_exp[warp][lane][w] = ex[w];
-            s_ev[warp][lane][w] = 0;
+        __syncwarp();
+        // ---- phase 2: bound test of the exposed words, one word per lane ----
+        for (int p = lane; p < total; p += 32) {
+          const int o = find_owner(S.off, p);
+          uint32_t m = S.cnt4[o];
+          for (int k = p - S.off[o]; k > 0; --k) m &= m - 1;
+          const int w = __ffs(m) - 1;
+          const int orow = T.row_begin + S.rloc[o];
+          const int ocol = S.col[o];
+          const int word = 4 * ocol + w;
+          const uint32_t Xw = S.X[o][w];
+          // every exposed replica has P <= x <= |bs_r| ef(e_max) =: B
+          float bsmax = c.beta_r ? s_bw[4 * (ocol - cbase) + w] : fabsf(c.beta);
+          if (c.sus) bsmax = __fmul_rn(bsmax, fabsf(c.sus[orow]));
+          const float B = __fmul_rn(bsmax, S.efmax[o]);
+          uint32_t Cw = 0;
+          uint32_t pl[8];
+          int have = 0;
+          if (B >= 1.0f) {
+            Cw = Xw;
+          } else if (B > 0.0f) {
+            Cw = sliced_less_word(Xw, fixed64(B), c.rk, (uint32_t)orow, step, (uint32_t)word,
+                                  kTagInfect, pl, have);
           }
-          __syncwarp();
-          for (int p = lane; p < total; p += 32) {
-            int owner = 0;
+          S.C[o][w] = Cw;
+          S.have[o][w] = (uint8_t)(have >= 4 ? 4 : 0);
+          if (have >= 4) {
 #pragma unroll
-            for (int st = 16; st > 0; st >>= 1)
-              if (owner + st < 32 && s_off[warp][owner + st] <= p) owner += st;
-            uint32_t m = s_qm[warp][owner];
-            for (int k = p - s_off[warp][owner]; k > 0; --k) m &= m - 1;
-            const int slot = __ffs(m) - 1;
-            const int w = slot >> 3, q = slot & 7;
-            const int orow = s_row[warp][owner];
-            const int word = 4 * s_col[warp][owner] + w;
-            const uint32_t bits = (s_exp[warp][owner][w] >> (4 * q)) & 0xFu;
-            long long e0 = 0, e1 = 0, e2 = 0, e3 = 0;
-            const int32_t ob = row_ptr[orow], oe = row_ptr[orow + 1];
-            for (int32_t k = ob; k < oe; ++k) {
-              const int2 en = ent[k];
-              const uint32_t mw = mask_w[(int64_t)en.x * L.words + word] >> (4 * q);
-              e0 += (mw & 1u) ? en.y : 0;
-              e1 += (mw & 2u) ? en.y : 0;
-              e2 += (mw & 4u) ? en.y : 0;
-              e3 += (mw & 8u) ? en.y : 0;
-            }
-            uint32_t x[4];
-            philox4x32_10((uint32_t)orow, step, (uint32_t)(word * 8 + q), kStreamInfect, c.key0,
-                          c.key1, x);
-            const float sus = c.sus ? c.sus[orow] : 1.0f;
-            const long long ev4[4] = {e0, e1, e2, e3};
-            uint32_t ev = 0;
-#pragma unroll
-            for (int cq = 0; cq < 4; ++cq) {
-              if ((bits >> cq) & 1u) {
-                const int r = word * 32 + 4 * q + cq;
-                const float br = c.beta_r ? c.beta_r[r] : c.beta;
-                const float bs = c.sus ? __fmul_rn(br, sus) : br;
-                float ef = __ll2float_rn(ev4[cq]);
-                if (scale != 1.0f) ef = __fmul_rn(ef, scale);
-                if (one_minus_exp_neg(__fmul_rn(bs, ef)) > unit24(x[cq]))
-                  ev |= 1u << (4 * q + cq);
-              }
-            }
-            if (ev) atomicOr(&s_ev[warp][owner][w], ev);
+            for (int q = 0; q < 4; ++q) S.pl[o][w][q] = pl[q];
           }
-          __syncwarp();
-#pragma unroll
-          for (int w = 0; w < 4; ++w) ex[w] = s_ev[warp][lane][w];
-          __syncwarp();
         }
-        if (nonempty && col_ok)
-          evs[(int64_t)row * L.q4 + col] = make_uint4(ex[0], ex[1], ex[2], ex[3]);
+        __syncwarp();
+        // ---- phase 3: exact test of the candidates, one replica per lane ----
+        const int ncand =
+            __popc(S.C[lane][0]) + __popc(S.C[lane][1]) + __popc(S.C[lane][2]) + __popc(S.C[lane][3]);
+        int ctotal;
+        const int coff = warp_excl_scan(ncand, lane, ctotal);
+        __syncwarp();
+        S.off[lane] = coff;
+        __syncwarp();
+        for (int p = lane; p < ctotal; p += 32) {
+          const int o = find_owner(S.off, p);
+          int w, b;
+          kth_bit4(S.C[o], p - S.off[o], w, b);
+          const int orl = S.rloc[o];
+          const int orow = T.row_begin + orl;
+          const int ocol = S.col[o];
+          const int word = 4 * ocol + w;
+          long long e = 0;
+          const int32_t ob = s_rp[orl], oe = s_rp[orl + 1];
+          for (int32_t k = ob; k < oe; ++k) {
+            const int2 q0 = staged ? s_ent[k - e0] : ent[k];
+            e += ((mask_w[(int64_t)q0.x * L.words + word] >> b) & 1u) ? q0.y : 0;
+          }
+          const float br = c.beta_r ? s_beta[(4 * (ocol - cbase) + w) * 32 + b] : c.beta;
+          const float bs = c.sus ? __fmul_rn(br, c.sus[orow]) : br;
+          float ef = __ll2float_rn(e);
+          if (scale != 1.0f) ef = __fmul_rn(ef, scale);
+          const float xx = __fmul_rn(bs, ef);
+          uint32_t pl[8];
+          const int have = S.have[o][w];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) pl[q] = S.pl[o][w][q];
+#pragma unroll
+          for (int q = 4; q < 8; ++q) pl[q] = 0;
+          // P <= x: a uniform at or above x cannot infect (no exponential)
+          if (xx > 0.0f && xx < 1.0f &&
+              !sliced_less_one((uint32_t)b, fixed64(xx), pl, have, c.rk, (uint32_t)orow, step,
+                               (uint32_t)word, kTagInfect))
+            continue;
+          if (infect_event(one_minus_exp_neg(xx), pl, have, c.rk, (uint32_t)orow, step,
+                           (uint32_t)word, (uint32_t)b))
+            atomicOr(&S.ev[o][w], 1u << b);
+        }
+        __syncwarp();
+        if (ok) {
+          const uint32_t v0 = S.ev[lane][0], v1 = S.ev[lane][1], v2 = S.ev[lane][2],
+                         v3 = S.ev[lane][3];
+          if (v0 | v1 | v2 | v3) {
+            const int64_t idx = (int64_t)row * L.q4 + col;
+            evs[idx] = make_uint4(v0, v1, v2, v3);
+            atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
+          }
+        }
+        __syncwarp();
       }
+      __syncthreads();
+      r0 = r1;
     }
   }
 }
@@ -210,98 +339,195 @@ __device__ __forceinline__ void count_bits(unsigned long long *s_ev, int wl, uin
   }
 }
 
-__global__ void __launch_bounds__(kThreads)
+// Applies one word's moves; returns the new planes and counts the events.
+__device__ __forceinline__ void apply_word(uint32_t A, uint32_t B, uint32_t evS, uint32_t f,
+                                           bool waning, const StepConsts &c,
+                                           unsigned long long *s_ev, int wl, uint32_t &na,
+                                           uint32_t &nb) {
+  const uint32_t E = ~A & B, I = A & ~B, Rw = waning ? (A & B) : 0u;
+  const uint32_t evE = f & E, evI = f & I, evR = f & Rw;
+  uint32_t xa = A, xb = B;
+  if (c.has_exposed)
+    xb |= evS;
+  else
+    xa |= evS;
+  xa |= evE;
+  xb &= ~evE;
+  if (c.ir_to_s)
+    xa &= ~evI;
+  else
+    xb |= evI;
+  xa &= ~evR;
+  xb &= ~evR;
+  na = xa;
+  nb = xb;
+  if (evS | evE | evI | evR) {
+    count_bits(s_ev, wl, c.has_exposed ? evS : 0u, 1ull);
+    count_bits(s_ev, wl, evE | (c.has_exposed ? 0u : evS), 1ull << 16);
+    count_bits(s_ev, wl, evI, 1ull << 32);
+    count_bits(s_ev, wl, evR, 1ull << 48);
+  }
+}
+
+// Per-warp queue of words with flow candidates (dynamic shared memory):
+// words are queued while the warp streams its items and drawn in full
+// 32-lane rounds, so sparse candidates do not leave lanes idle.
+struct FlowQueue {
+  int32_t row[64];
+  int32_t word[64];
+  uint32_t a0[64], b0[64];  // planes at the start of the step
+  uint32_t evs[64];         // the word's infection events
+  int32_t wl[64];           // word index within the slice (counters)
+  int32_t n;
+};
+constexpr int kFlowDynSmem = 128 * 32 * 8 + kWarps * (int)sizeof(FlowQueue);
+
+// Draws the flows of queue entries [0, cnt) (cnt <= 32, one per lane) and
+// writes the words: infection events and flows act on disjoint state bits,
+// so both are applied here from the start-of-step planes.
+__device__ __forceinline__ void flow_round(FlowQueue &Q, int cnt, int lane, bool waning,
+                                           const StepConsts &c, uint32_t step,
+                                           unsigned long long *s_ev, uint32_t *sa_w,
+                                           uint32_t *sb_w, uint32_t *mask_w, int words) {
+  if (lane < cnt) {
+    const uint32_t A = Q.a0[lane], B = Q.b0[lane];
+    const uint32_t E = ~A & B, I = A & ~B, R = waning ? (A & B) : 0u;
+    const int row = Q.row[lane], word = Q.word[lane];
+    const uint32_t f = flow_events(E, I, R, c.th, c.rk, (uint32_t)row, step, (uint32_t)word);
+    uint32_t na, nb;
+    apply_word(A, B, Q.evs[lane], f, waning, c, s_ev, Q.wl[lane], na, nb);
+    if (na != A || nb != B) {
+      const int64_t wi = (int64_t)row * words + word;
+      sa_w[wi] = na;
+      sb_w[wi] = nb;
+      mask_w[wi] = na & ~nb;
+    }
+  }
+}
+
+// Streams the items of each task: infection events of words without flow
+// candidates are applied on the spot, words with candidates are queued.
+__global__ void __launch_bounds__(kThreads, 3)
     k_flow(PackedLayout L, const PackedTask *__restrict__ tasks,
-           const int32_t *__restrict__ row_ptr, const uint4 *__restrict__ evs,
-           uint4 *__restrict__ mask_out, uint4 *__restrict__ sa, uint4 *__restrict__ sb,
-           unsigned long long *__restrict__ ev_row, unsigned long long *__restrict__ rs_row,
-           uint32_t step, StepConsts c) {
-  // per task: 128 words x 32 replicas of 4 x 16-bit event counters
-  __shared__ unsigned long long s_ev[128 * 32];
+           const int32_t *__restrict__ row_ptr, uint4 *__restrict__ evs,
+           uint4 *__restrict__ mask, uint4 *__restrict__ sa, uint4 *__restrict__ sb,
+           uint8_t *__restrict__ flag, unsigned long long *__restrict__ ev_row,
+           unsigned long long *__restrict__ rs_row, uint32_t step, StepConsts c) {
+  extern __shared__ __align__(16) unsigned char s_dynf[];
+  // 4 x 16-bit event counters per replica of the slice
+  unsigned long long *s_ev = reinterpret_cast<unsigned long long *>(s_dynf);
+  FlowQueue &Q = reinterpret_cast<FlowQueue *>(s_dynf + 128 * 32 * 8)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int lpr = L.lpr, rpw = 32 / lpr;
-  const int rsub = lane / lpr, csub = lane % lpr;
   const bool waning = c.th.tr_all || c.th.tr != 0;
-  const unsigned long long kSE = 1ull, kXI = 1ull << 16, kIX = 1ull << 32, kRS = 1ull << 48;
+  uint32_t *sa_w = reinterpret_cast<uint32_t *>(sa);
+  uint32_t *sb_w = reinterpret_cast<uint32_t *>(sb);
+  uint32_t *mask_w = reinterpret_cast<uint32_t *>(mask);
   for (int ti = blockIdx.x; ti < L.n_tasks; ti += gridDim.x) {
     const PackedTask T = tasks[ti];
     const int cbase = T.slice * 32;
     const int ncols = min(32, L.q4 - cbase);
+    const Div dv((uint32_t)ncols);
+    const int nrows = T.row_end - T.row_begin;
     for (int j = threadIdx.x; j < 128 * 32; j += blockDim.x) s_ev[j] = 0;
+    if (lane == 0) Q.n = 0;
     __syncthreads();
-    for (int base = T.row_begin + warp * rpw; base < T.row_end; base += kWarps * rpw) {
-      const int row = base + rsub;
-      if (row >= T.row_end) continue;
-      const bool nonempty = row_ptr[row + 1] > row_ptr[row];
-      for (int cc = csub; cc < ncols; cc += lpr) {
-        const int col = cbase + cc;
-        const int64_t idx = (int64_t)row * L.q4 + col;
-        const uint4 a4 = sa[idx], b4 = sb[idx];
-        const uint4 e4 = nonempty ? evs[idx] : make_uint4(0, 0, 0, 0);
-        uint32_t na[4], nb[4], mo[4];
+    const int nitems = nrows * ncols;
+    for (int it0 = warp * 64; it0 < nitems; it0 += kWarps * 64) {  // warp-uniform
+      int rl[2], cl[2];
+      bool in[2];
+      uint8_t st[2];
+      uint4 a4[2], b4[2], e4[2];
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
-          const int word = 4 * col + w;
-          const uint32_t a = get4(a4, w), b = get4(b4, w);
-          na[w] = a;
-          nb[w] = b;
-          mo[w] = 0;
-          if (!word_mask(L, word)) continue;
-          const uint32_t E = ~a & b, I = a & ~b, R = a & b;
-          const uint32_t evS = get4(e4, w);
-          const uint32_t Rw = waning ? R : 0u;
-          const uint32_t evF =
-              (E | I | Rw) ? flow_events(E, I, Rw, c.th, c.key0, c.key1, (uint32_t)row, step,
-                                         (uint32_t)word)
-                           : 0u;
-          const uint32_t evE = evF & E, evI = evF & I, evR = evF & Rw;
-          uint32_t xa = a, xb = b;
-          if (c.has_exposed)
-            xb |= evS;
-          else
-            xa |= evS;
-          xa |= evE;
-          xb &= ~evE;
-          if (c.ir_to_s)
-            xa &= ~evI;
-          else
-            xb |= evI;
-          xa &= ~evR;
-          xb &= ~evR;
-          na[w] = xa;
-          nb[w] = xb;
-          mo[w] = xa & ~xb;
-          const int wl = 4 * cc + w;
-          if (evS | evE | evI | evR) {
-            count_bits(s_ev, wl, c.has_exposed ? evS : 0u, kSE);
-            count_bits(s_ev, wl, evE | (c.has_exposed ? 0u : evS), kXI);
-            count_bits(s_ev, wl, evI, kIX);
-            count_bits(s_ev, wl, evR, kRS);
+      for (int h = 0; h < 2; ++h) {
+        const int itv = it0 + 32 * h + lane;
+        in[h] = itv < nitems;
+        rl[h] = in[h] ? (int)dv.div((uint32_t)itv) : 0;
+        cl[h] = in[h] ? itv - rl[h] * ncols : 0;
+        const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
+        a4[h] = b4[h] = e4[h] = make_uint4(0, 0, 0, 0);
+        st[h] = 0;
+        if (in[h]) {
+          st[h] = flag[idx];
+          a4[h] = sa[idx];
+          b4[h] = sb[idx];
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        if (st[h]) {
+          const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
+          e4[h] = evs[idx];
+          evs[idx] = make_uint4(0, 0, 0, 0);
+          flag[idx] = 0;
+        }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int h = k >> 2, w = k & 3;
+        const uint32_t A = get4(a4[h], w), B = get4(b4[h], w), ev = get4(e4[h], w);
+        const int word = 4 * (cbase + cl[h]) + w;
+        const bool valid = in[h] && word_mask(L, word) != 0u;
+        const bool cand = valid && (waning ? (A | B) : (A ^ B)) != 0u;
+        // queue the candidate words of this slot across the warp
+        const unsigned qm = __ballot_sync(kFull, cand);
+        if (qm) {
+          const int base = Q.n;
+          const int pos = base + __popc(qm & ((1u << lane) - 1u));
+          if (cand) {
+            Q.row[pos] = T.row_begin + rl[h];
+            Q.word[pos] = word;
+            Q.a0[pos] = A;
+            Q.b0[pos] = B;
+            Q.evs[pos] = ev;
+            Q.wl[pos] = 4 * cl[h] + w;
+          }
+          __syncwarp();
+          if (lane == 0) Q.n = base + __popc(qm);
+          __syncwarp();
+          if (Q.n >= 32) {
+            flow_round(Q, 32, lane, waning, c, step, s_ev, sa_w, sb_w, mask_w, L.words);
+            __syncwarp();
+            const int rest = Q.n - 32;
+            if (lane < rest) {
+              Q.row[lane] = Q.row[32 + lane];
+              Q.word[lane] = Q.word[32 + lane];
+              Q.a0[lane] = Q.a0[32 + lane];
+              Q.b0[lane] = Q.b0[32 + lane];
+              Q.evs[lane] = Q.evs[32 + lane];
+              Q.wl[lane] = Q.wl[32 + lane];
+            }
+            __syncwarp();
+            if (lane == 0) Q.n = rest;
+            __syncwarp();
           }
         }
-        const uint4 oa = make_uint4(na[0], na[1], na[2], na[3]);
-        const uint4 ob = make_uint4(nb[0], nb[1], nb[2], nb[3]);
-        if (oa.x != a4.x || oa.y != a4.y || oa.z != a4.z || oa.w != a4.w) sa[idx] = oa;
-        if (ob.x != b4.x || ob.y != b4.y || ob.z != b4.z || ob.w != b4.w) sb[idx] = ob;
-        mask_out[idx] = make_uint4(mo[0], mo[1], mo[2], mo[3]);
+        // infection events of a word without flow candidates: apply now
+        if (valid && !cand && ev) {
+          uint32_t na, nb;
+          apply_word(A, B, ev, 0u, waning, c, s_ev, 4 * cl[h] + w, na, nb);
+          const int64_t wi = (int64_t)(T.row_begin + rl[h]) * L.words + word;
+          sa_w[wi] = na;
+          sb_w[wi] = nb;
+          mask_w[wi] = na & ~nb;
+        }
       }
     }
+    __syncwarp();
+    flow_round(Q, Q.n, lane, waning, c, step, s_ev, sa_w, sb_w, mask_w, L.words);
     __syncthreads();
     for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x) {
       const unsigned long long v = s_ev[j];
       if (!v) continue;
       const int rep = cbase * 128 + j;
       if (rep >= L.m) continue;
-      const unsigned long long f = 0xFFFFull;
-      const unsigned long long g = (v & f) | (((v >> 16) & f) << kFieldBits) |
-                                   (((v >> 32) & f) << (2 * kFieldBits));
+      const unsigned long long f16 = 0xFFFFull;
+      const unsigned long long g = (v & f16) | (((v >> 16) & f16) << kFieldBits) |
+                                   (((v >> 32) & f16) << (2 * kFieldBits));
       if (g) atomicAdd(&ev_row[T.count_base + rep], g);
       if (rs_row && (v >> 48)) atomicAdd(&rs_row[T.count_base + rep], v >> 48);
     }
     __syncthreads();
   }
 }
-
 // Full E/I/R counts of the planes (initial state): one shared atomic per
 // set bit, E | I << 21 | R << 42 per replica.
 __global__ void __launch_bounds__(kThreads)
@@ -469,9 +695,19 @@ int task_grid(int n_tasks, int per_sm) {
 
 }  // namespace
 
-void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb, uint32_t *mask, float p0,
-                 int32_t k_exact, const int32_t *net_first_row, const int32_t *net_rows,
-                 int32_t n_nets, const StepConsts &c, cudaStream_t st) {
+rp_status packed_prepare() {
+  cudaError_t e = cudaFuncSetAttribute(k_flow, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kFlowDynSmem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_flow)");
+  e = cudaFuncSetAttribute(k_infect, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfectDynSmem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_infect)");
+  return RP_OK;
+}
+
+void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb, uint32_t *mask,
+                 uint8_t *flag, float p0, int32_t k_exact, const int32_t *net_first_row,
+                 const int32_t *net_rows, int32_t n_nets, const StepConsts &c,
+                 cudaStream_t st) {
   const int64_t total = (int64_t)L.n_nodes * L.words;
   k_packed_init<<<1184, 256, 0, st>>>(L, sa, sb, mask, k_exact > 0 ? 0.0f : p0, c);
   if (k_exact > 0) {
@@ -480,20 +716,35 @@ void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb, uint32_t *ma
                                                                 n_nets, k_exact, c);
     k_mask_from_planes<<<1184, 256, 0, st>>>(total, sa, sb, mask);
   }
+  cudaMemsetAsync(flag, 0, ((size_t)L.n_nodes * L.q4 + 3) / 4 * 4, st);
 }
 
 void packed_step(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
-                 const int2 *entries, const uint32_t *mask_in, uint32_t *mask_out, uint32_t *sa,
-                 uint32_t *sb, uint32_t *evs, unsigned long long *ev_row,
-                 unsigned long long *rs_row, uint32_t step, float scale, const StepConsts &c,
-                 cudaStream_t st) {
-  k_infect<<<task_grid(L.n_tasks, 4), kThreads, 0, st>>>(
-      L, tasks, row_ptr, entries, reinterpret_cast<const uint4 *>(mask_in),
+                 const int2 *entries, uint32_t *mask, uint32_t *sa, uint32_t *sb, uint32_t *evs,
+                 uint8_t *flag, unsigned long long *ev_row, unsigned long long *rs_row,
+                 uint32_t step, float scale, const StepConsts &c, cudaStream_t st) {
+  packed_infect(L, tasks, row_ptr, entries, mask, sa, sb, evs, flag, step, scale, c, st);
+  packed_flow(L, tasks, row_ptr, mask, sa, sb, evs, flag, ev_row, rs_row, step, c, st);
+}
+
+void packed_infect(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
+                   const int2 *entries, const uint32_t *mask, const uint32_t *sa,
+                   const uint32_t *sb, uint32_t *evs, uint8_t *flag, uint32_t step, float scale,
+                   const StepConsts &c, cudaStream_t st) {
+  k_infect<<<task_grid(L.n_tasks, 3), kThreads, kInfectDynSmem, st>>>(
+      L, tasks, row_ptr, entries, reinterpret_cast<const uint4 *>(mask),
       reinterpret_cast<const uint4 *>(sa), reinterpret_cast<const uint4 *>(sb),
-      reinterpret_cast<uint4 *>(evs), step, scale, c);
-  k_flow<<<task_grid(L.n_tasks, 4), kThreads, 0, st>>>(
-      L, tasks, row_ptr, reinterpret_cast<const uint4 *>(evs), reinterpret_cast<uint4 *>(mask_out),
-      reinterpret_cast<uint4 *>(sa), reinterpret_cast<uint4 *>(sb), ev_row, rs_row, step, c);
+      reinterpret_cast<uint4 *>(evs), reinterpret_cast<uint32_t *>(flag), step, scale, c);
+}
+
+void packed_flow(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
+                 uint32_t *mask, uint32_t *sa, uint32_t *sb, const uint32_t *evs, uint8_t *flag,
+                 unsigned long long *ev_row, unsigned long long *rs_row, uint32_t step,
+                 const StepConsts &c, cudaStream_t st) {
+  k_flow<<<task_grid(L.n_tasks, 3), kThreads, kFlowDynSmem, st>>>(
+      L, tasks, row_ptr, reinterpret_cast<uint4 *>(const_cast<uint32_t *>(evs)),
+      reinterpret_cast<uint4 *>(mask), reinterpret_cast<uint4 *>(sa),
+      reinterpret_cast<uint4 *>(sb), flag, ev_row, rs_row, step, c);
 }
 
 void packed_count(const PackedLayout &L, const PackedTask *tasks, const uint32_t *sa,

@@ -166,7 +166,6 @@ __global__ void __launch_bounds__(256)
     uint8_t v[4];
     int64_t e[4];
     uint32_t Em = 0, Im = 0, Rm = 0;
-    bool any_exposed = false;
 #pragma unroll
     for (int c4 = 0; c4 < 4; ++c4) {
       const int32_t r = 4 * q + c4;
@@ -176,18 +175,16 @@ __global__ void __launch_bounds__(256)
         const int64_t idx = i + (int64_t)r * n;
         v[c4] = st[idx];
         if (v[c4] == 0) e[c4] = expo[idx];
-        any_exposed |= v[c4] == 0 && e[c4] > 0;
         const uint32_t bit = 1u << (r & 31);
         Em |= v[c4] == 1 ? bit : 0u;
         Im |= v[c4] == 2 ? bit : 0u;
         Rm |= v[c4] == 3 ? bit : 0u;
       }
     }
-    uint32_t x[4] = {0, 0, 0, 0};
-    if (any_exposed)
-      philox4x32_10((uint32_t)i, step, (uint32_t)q, kStreamInfect, c.key0, c.key1, x);
+    const uint32_t word = (uint32_t)(q >> 3);
+    const uint32_t no_planes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const uint32_t ev = (Em | Im | Rm)
-                            ? flow_events(Em, Im, Rm, c.th, c.key0, c.key1, (uint32_t)i, step,
+                            ? flow_events(Em, Im, Rm, c.th, c.rk, (uint32_t)i, step,
                                           (uint32_t)(q >> 3))
                             : 0u;
 #pragma unroll
@@ -199,7 +196,8 @@ __global__ void __launch_bounds__(256)
       if (v[c4] == 0) {
         if (e[c4] > 0) {
           const float P = one_minus_exp_neg(infection_x(c, r, i, e[c4], scale));
-          if (P > unit24(x[c4])) nv = c.has_exposed ? 1 : 2;
+          if (infect_event(P, no_planes, 0, c.rk, (uint32_t)i, step, word, (uint32_t)(r & 31)))
+            nv = c.has_exposed ? 1 : 2;
         }
       } else if (v[c4] == 1) {
         if (fired) nv = 2;

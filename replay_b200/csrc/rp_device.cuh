@@ -36,6 +36,30 @@ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1,
   out[3] = c3;
 }
 
+// Same generator with the 10 round keys precomputed (key schedule hoisted
+// out of the per-call work): rk[2 i], rk[2 i + 1] are round i's key words.
+__device__ __forceinline__ void philox4x32_10_rk(uint32_t c0, uint32_t c1, uint32_t c2,
+                                                 uint32_t c3, const uint32_t *rk,
+                                                 uint32_t out[4]) {
+#pragma unroll
+  for (int round = 0; round < 10; ++round) {
+    const uint32_t lo0 = 0xD2511F53u * c0;
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2);
+    const uint32_t n0 = hi1 ^ c1 ^ rk[2 * round];
+    const uint32_t n2 = hi0 ^ c3 ^ rk[2 * round + 1];
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
 // Uniform on the 24-bit grid ((x >> 8) + 1) * 2^-24, in (0, 1]; exact in
 // float, so host and device agree bit for bit.
 __device__ __forceinline__ float unit24(uint32_t x) {
@@ -99,17 +123,18 @@ __device__ __forceinline__ float one_minus_exp_neg(float x) {
 // random plane per bit, stopping when every candidate is decided (about
 // log2(candidates) + 2 planes).  Returns the event mask.
 __device__ __forceinline__ uint32_t flow_events(uint32_t E, uint32_t I, uint32_t R,
-                                                const FlowThresholds &th, uint32_t key0,
-                                                uint32_t key1, uint32_t node, uint32_t step,
-                                                uint32_t word) {
+                                                const FlowThresholds &th, const uint32_t *rk,
+                                                uint32_t node, uint32_t step, uint32_t word) {
   uint32_t lt = (th.te_all ? E : 0u) | (th.ti_all ? I : 0u) | (th.tr_all ? R : 0u);
   const uint32_t e2 = (th.te_all || th.te == 0) ? 0u : E;
   const uint32_t i2 = (th.ti_all || th.ti == 0) ? 0u : I;
   const uint32_t r2 = (th.tr_all || th.tr == 0) ? 0u : R;
   uint32_t und = e2 | i2 | r2;
-  for (int j = 0; und != 0u && j < 16; ++j) {
+  // the first two calls (8 planes) run unconditionally so that lanes stay in
+  // step; later planes only while some replica is undecided
+  for (int j = 0; j < 16 && (j < 2 || und != 0u); ++j) {
     uint32_t x[4];
-    philox4x32_10(node, step, word, (uint32_t)j << 4, key0, key1, x);
+    philox4x32_10_rk(node, step, word, (uint32_t)j << 4, rk, x);
     const int sh = 60 - 4 * j;
     const uint32_t ce = (uint32_t)(th.te >> sh) & 0xFu;
     const uint32_t ci = (uint32_t)(th.ti >> sh) & 0xFu;
@@ -125,6 +150,83 @@ __device__ __forceinline__ uint32_t flow_events(uint32_t E, uint32_t I, uint32_t
     }
   }
   return lt;
+}
+
+// floor(p 2^64) for 0 < p < 1 (exact: p 2^64 is exact in float, then
+// truncated).
+__device__ __forceinline__ unsigned long long fixed64(float p) {
+  return __float2ull_rz(__fmul_rn(p, 0x1p64f));
+}
+
+// Bit-sliced comparison of the uniforms of the replicas in `cand` (one
+// 32-replica word) with one 64-bit threshold: bit k of U_r is bit r of
+// output k % 4 of counter (node, step, word, tag | (k / 4) << 4).  Returns
+// the replicas with U_r < T; the first 8 planes are kept in pl (*have of
+// them generated) for follow-up comparisons.
+__device__ __forceinline__ uint32_t sliced_less_word(uint32_t cand, unsigned long long T,
+                                                     const uint32_t *rk, uint32_t node,
+                                                     uint32_t step, uint32_t word, uint32_t tag,
+                                                     uint32_t pl[8], int &have) {
+  uint32_t lt = 0, und = cand;
+  have = 0;
+  for (int j = 0; j < 16 && (j < 2 || und != 0u); ++j) {
+    uint32_t x[4];
+    philox4x32_10_rk(node, step, word, tag | ((uint32_t)j << 4), rk, x);
+    if (j == 0) {
+      pl[0] = x[0]; pl[1] = x[1]; pl[2] = x[2]; pl[3] = x[3];
+      have = 4;
+    } else if (j == 1) {
+      pl[4] = x[0]; pl[5] = x[1]; pl[6] = x[2]; pl[7] = x[3];
+      have = 8;
+    }
+    const uint32_t chunk = (uint32_t)(T >> (60 - 4 * j)) & 0xFu;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t t = ((chunk >> (3 - q)) & 1u) ? 0xFFFFFFFFu : 0u;
+      const uint32_t w = x[q];
+      lt |= und & t & ~w;
+      und &= ~(t ^ w);
+    }
+  }
+  return lt;
+}
+
+// U_b < Pf for one replica bit b of the word, first from the kept planes,
+// then from fresh ones.
+__device__ __forceinline__ bool sliced_less_one(uint32_t b, unsigned long long Pf,
+                                                const uint32_t pl[8], int have,
+                                                const uint32_t *rk, uint32_t node, uint32_t step,
+                                                uint32_t word, uint32_t tag) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (k >= have) break;
+    const uint32_t wb = (pl[k] >> b) & 1u;
+    const uint32_t tb = (uint32_t)(Pf >> (63 - k)) & 1u;
+    if (wb != tb) return wb < tb;
+  }
+  for (int j = have / 4; j < 16; ++j) {
+    uint32_t x[4];
+    philox4x32_10_rk(node, step, word, tag | ((uint32_t)j << 4), rk, x);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = 4 * j + q;
+      const uint32_t wb = (x[q] >> b) & 1u;
+      const uint32_t tb = (uint32_t)(Pf >> (63 - k)) & 1u;
+      if (wb != tb) return wb < tb;
+    }
+  }
+  return false;
+}
+
+// Geometric infection decision of replica bit b: its uniform is bit-sliced
+// on tag 4; event iff U < floor(P 2^64) (P >= 1 always, P <= 0 or NaN never).
+constexpr uint32_t kTagInfect = 4u;
+__device__ __forceinline__ bool infect_event(float P, const uint32_t pl[8], int have,
+                                             const uint32_t *rk, uint32_t node, uint32_t step,
+                                             uint32_t word, uint32_t b) {
+  if (!(P > 0.0f)) return false;
+  if (P >= 1.0f) return true;
+  return sliced_less_one(b, fixed64(P), pl, have, rk, node, step, word, kTagInfect);
 }
 
 // Countdown arithmetic of the reference (int op float, truncated back to

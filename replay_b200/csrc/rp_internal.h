@@ -159,6 +159,7 @@ void enqueue_window_compact(WindowWorkspace &ws, int32_t *row_ptr_out,
 // ---- kernels of the step loop -------------------------------------------------
 struct StepConsts {
   uint32_t key0, key1;
+  uint32_t rk[20];    // Philox round keys of (key0, key1)
   FlowThresholds th;  // p_ei, p_ir, p_rs as 64-bit fixed point
   float step_size;
   float neg_log_base;  // -logf(1 - infect_prob), countdown mode
@@ -202,16 +203,28 @@ struct PackedLayout {
   int32_t lpr;        // lanes per row (power of 2, <= 32)
   int32_t n_tasks;
 };
+rp_status packed_prepare();  // kernel attributes, once per device
 void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb,
-                 uint32_t *mask, float p0, int32_t k_exact,
+                 uint32_t *mask, uint8_t *flag, float p0, int32_t k_exact,
                  const int32_t *net_first_row, const int32_t *net_rows,
                  int32_t n_nets, const StepConsts &c, cudaStream_t st);
 void packed_step(const PackedLayout &L, const PackedTask *tasks,
-                 const int32_t *row_ptr, const int2 *entries,
-                 const uint32_t *mask_in, uint32_t *mask_out, uint32_t *sa,
-                 uint32_t *sb, uint32_t *evs, unsigned long long *ev_row,
-                 unsigned long long *rs_row, uint32_t step, float scale,
-                 const StepConsts &c, cudaStream_t st);
+                 const int32_t *row_ptr, const int2 *entries, uint32_t *mask,
+                 uint32_t *sa, uint32_t *sb, uint32_t *evs, uint8_t *flag,
+                 unsigned long long *ev_row, unsigned long long *rs_row,
+                 uint32_t step, float scale, const StepConsts &c,
+                 cudaStream_t st);
+// The two halves of packed_step (exposure + infection draws; transitions).
+void packed_infect(const PackedLayout &L, const PackedTask *tasks,
+                   const int32_t *row_ptr, const int2 *entries,
+                   const uint32_t *mask, const uint32_t *sa, const uint32_t *sb,
+                   uint32_t *evs, uint8_t *flag, uint32_t step, float scale,
+                   const StepConsts &c, cudaStream_t st);
+void packed_flow(const PackedLayout &L, const PackedTask *tasks,
+                 const int32_t *row_ptr, uint32_t *mask, uint32_t *sa,
+                 uint32_t *sb, const uint32_t *evs, uint8_t *flag,
+                 unsigned long long *ev_row, unsigned long long *rs_row,
+                 uint32_t step, const StepConsts &c, cudaStream_t st);
 void packed_count(const PackedLayout &L, const PackedTask *tasks,
                   const uint32_t *sa, const uint32_t *sb,
                   unsigned long long *counts_row, cudaStream_t st);
