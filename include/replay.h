@@ -79,6 +79,20 @@ RP_API rp_status rp_graph_from_arrays(const int64_t *start, const int64_t *end,
                                       int64_t n_contacts, int32_t n_nodes,
                                       int device, rp_graph **out);
 
+/* Parses a contact file into host arrays only (no device is touched), with
+ * the same rules as rp_graph_load_text: u[k] <= v[k] are compressed node
+ * indices in order of first appearance, start/end in Unix seconds, file
+ * order kept.  The four arrays are allocated by the library (NULL when
+ * *n_contacts is 0) and released with rp_free.
+ * Replaces parse_edgelist_build_intervals
+ * (tool/temporal_contact_matrix.c:148-321). */
+RP_API rp_status rp_parse_contacts(const char *path, int32_t *n_nodes,
+                                   int32_t *n_index, int64_t *n_contacts,
+                                   int64_t *n_malformed, int64_t **start,
+                                   int64_t **end, int32_t **u, int32_t **v);
+/* Releases an array returned by rp_parse_contacts. */
+RP_API void rp_free(void *p);
+
 RP_API rp_status rp_graph_get_info(const rp_graph *g, rp_graph_info *out);
 
 /* Frees the graph.  Replaces free_interval_db_wrapper + free_node_map

@@ -147,6 +147,13 @@ def sorted_index(start, end, u, v):
     return ss, se, np.asarray(u, np.int32)[perm].copy(), np.asarray(v, np.int32)[perm].copy(), perm, nlists(ss, se)
 
 
+def hit_coords(s, e, ws):
+    """Coordinates a stored hit (s, e) is handed to the CSR builder with."""
+    hs, he = C.c_int64(), C.c_int64()
+    lib().orc_hit_coords(C.c_int64(int(s)), C.c_int64(int(e)), C.c_int64(int(ws)), C.byref(hs), C.byref(he))
+    return hs.value, he.value
+
+
 def sort_order(start, end):
     start = np.ascontiguousarray(start, np.int64)
     end = np.ascontiguousarray(end, np.int64)

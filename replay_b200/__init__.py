@@ -22,7 +22,7 @@ import numpy as np
 from . import _lib
 from ._lib import CLI_PATH, ReplayError, check, lib
 
-__all__ = ["Graph", "Simulation", "ReplayError", "window_csr", "CLI_PATH", "version"]
+__all__ = ["Graph", "Simulation", "ReplayError", "window_csr", "parse_contacts", "CLI_PATH", "version"]
 
 
 def version():
@@ -31,6 +31,34 @@ def version():
 
 def _ptr(a):
     return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def parse_contacts(path):
+    """Parses a contact file on the host (no GPU work).
+
+    Returns dict(n_nodes, n_index, n_malformed, start, end, u, v): int64
+    Unix-second intervals and int32 compressed node indices (u <= v, order of
+    first appearance), in file order.  Raises ReplayError where the reference
+    parser fails (unreadable file, bad NODE_LIST header, no contacts).
+    """
+    L = lib()
+    nn, ni = C.c_int32(), C.c_int32()
+    nc, nm = C.c_int64(), C.c_int64()
+    ps, pe, pu, pv = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+    check(L.rp_parse_contacts(str(path).encode(), C.byref(nn), C.byref(ni), C.byref(nc), C.byref(nm),
+                              C.byref(ps), C.byref(pe), C.byref(pu), C.byref(pv)))
+    n = nc.value
+
+    def take(p, ctype, dtype):
+        if n == 0:
+            return np.zeros(0, dtype)
+        arr = np.ctypeslib.as_array(C.cast(p, C.POINTER(ctype)), shape=(n,)).astype(dtype)
+        L.rp_free(p)
+        return arr
+
+    return {"n_nodes": nn.value, "n_index": ni.value, "n_malformed": nm.value,
+            "start": take(ps, C.c_int64, np.int64), "end": take(pe, C.c_int64, np.int64),
+            "u": take(pu, C.c_int32, np.int32), "v": take(pv, C.c_int32, np.int32)}
 
 
 class Graph:

@@ -79,6 +79,10 @@ SIGNATURES = {
     "rp_graph_load_text": ([C.c_char_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "rp_graph_from_arrays": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int,
                               C.POINTER(C.c_void_p)], C.c_int),
+    "rp_parse_contacts": ([C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                           C.POINTER(C.c_int64), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                           C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)], C.c_int),
+    "rp_free": ([C.c_void_p], None),
     "rp_graph_get_info": ([C.c_void_p, C.POINTER(GraphInfo)], C.c_int),
     "rp_graph_free": ([C.c_void_p], None),
     "rp_window_csr": ([C.c_void_p, C.c_int64, C.c_int64, C.c_float, C.c_int32, C.c_int32, C.c_void_p,

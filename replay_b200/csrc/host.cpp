@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -537,6 +538,46 @@ RP_API rp_status rp_graph_load_text(const char *path, int device, rp_graph **out
   *out = h.release();
   return RP_OK;
 }
+
+RP_API rp_status rp_parse_contacts(const char *path, int32_t *n_nodes, int32_t *n_index,
+                                   int64_t *n_contacts, int64_t *n_malformed, int64_t **start,
+                                   int64_t **end, int32_t **u, int32_t **v) {
+  if (!path || !n_nodes || !n_index || !n_contacts || !n_malformed || !start || !end || !u || !v) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  *start = *end = nullptr;
+  *u = *v = nullptr;
+  *n_contacts = 0;
+  std::vector<int64_t> st, en;
+  std::vector<int32_t> uu, vv;
+  int32_t nn = 0, ni = 0;
+  int64_t malformed = 0;
+  RP_TRY(parse_contact_file(path, nn, ni, malformed, st, en, uu, vv));
+  *n_nodes = nn;
+  *n_index = ni;
+  *n_malformed = malformed;
+  const size_t n = st.size();
+  if (n == 0) return RP_OK;
+  int64_t *ps = (int64_t *)malloc(n * sizeof(int64_t));
+  int64_t *pe = (int64_t *)malloc(n * sizeof(int64_t));
+  int32_t *pu = (int32_t *)malloc(n * sizeof(int32_t));
+  int32_t *pv = (int32_t *)malloc(n * sizeof(int32_t));
+  if (!ps || !pe || !pu || !pv) {
+    free(ps), free(pe), free(pu), free(pv);
+    set_error("out of host memory for %zu contacts", n);
+    return RP_ERR_NOMEM;
+  }
+  memcpy(ps, st.data(), n * sizeof(int64_t));
+  memcpy(pe, en.data(), n * sizeof(int64_t));
+  memcpy(pu, uu.data(), n * sizeof(int32_t));
+  memcpy(pv, vv.data(), n * sizeof(int32_t));
+  *start = ps, *end = pe, *u = pu, *v = pv;
+  *n_contacts = (int64_t)n;
+  return RP_OK;
+}
+
+RP_API void rp_free(void *p) { free(p); }
 
 RP_API rp_status rp_graph_from_arrays(const int64_t *start, const int64_t *end,
                                       const int32_t *u, const int32_t *v, int64_t n_contacts,
