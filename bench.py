@@ -37,7 +37,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sweep", "small"], default="sweep")
+    ap.add_argument("--workload", choices=["sweep", "small", "hot"], default="sweep",
+                    help="sweep: the replica-sweep replay (default); small: N=1,000 / 1,000 replicas; "
+                         "hot: the sweep network with 5,000 initial infected for 12 steps (profiler case)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain-path / CPU / e2e legs")
     return ap.parse_args()
 
@@ -102,7 +104,29 @@ class ClockSampler:
 
 def workload(name):
     from replay_b200 import synthetic
-    return synthetic.replica_sweep() if name == "sweep" else synthetic.small_seir()
+    if name == "small":
+        return synthetic.small_seir()
+    net = synthetic.replica_sweep()
+    if name == "hot":
+        # every step as busy as the sweep's peak: a short replay for profiler captures
+        net["params"] = dict(net["params"], initial_count=5000, iterations=12)
+        net["name"] += " (5,000 initial infected, 12 steps)"
+    return net
+
+
+def profiled_traffic(name):
+    """DRAM bytes per step (both step kernels) from the committed ncu summary of
+    this workload, or None: lines `traffic_bytes_per_step <workload> <bytes>`."""
+    path = os.path.join(ROOT, "profiles", "launches_replica_sweep.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.strip().strip("`").split()
+                if len(parts) == 3 and parts[0] == "traffic_bytes_per_step" and parts[1] == name:
+                    return float(parts[2])
+    except OSError:
+        pass
+    return None
 
 
 def algorithmic_bytes(n, m, steps, nnz_total):
@@ -138,9 +162,7 @@ def run_ours(args, rank, world, local_rank):
     g = replay_b200.Graph.from_arrays(net["start"], net["end"], net["u"], net["v"], n_nodes, device=dev)
     ingest_s = time.perf_counter() - t0
     sim = replay_b200.Simulation(g, path="batched", csr="per-step", **p)
-    sim_pre = replay_b200.Simulation(g, path="batched", csr="prebuilt", **p)
     info = sim.info
-    info_pre = sim_pre.info
 
     stream = torch.cuda.Stream(device=dev)
 
@@ -180,24 +202,32 @@ def run_ours(args, rank, world, local_rank):
            "clocks": clocks,
            "gpu_launches": info["kernels_per_run"] * args.steps}
 
-    # ---- prebuilt-CSR variant ----
-    ms_pre = timed(sim_pre, args.steps, 1) / args.steps
-    out["prebuilt_csr"] = {"value": nrs_per_replay * world / (ms_pre / 1e3), "ms_per_step": ms_pre,
-                           "prebuilt_nnz": info_pre["prebuilt_nnz"]}
+    # ---- prebuilt-CSR variant (with --no-extras only built, for its nnz count,
+    # after the per-step replays, so that those are the process's first launches) ----
+    prof_ps = sim.profile() if args.no_extras else None
+    sim_pre = replay_b200.Simulation(g, path="batched", csr="prebuilt", **p)
+    nnz_total = sim_pre.info["nnz_total"]
+    if not args.no_extras:
+        ms_pre = timed(sim_pre, args.steps, 1) / args.steps
+        out["prebuilt_csr"] = {"value": nrs_per_replay * world / (ms_pre / 1e3), "ms_per_step": ms_pre,
+                               "prebuilt_nnz": sim_pre.info["prebuilt_nnz"]}
 
-    # ---- roofline of the dominant kernel (k_packed_step) ----
+    # ---- roofline of the step: k_infect + k_flow, one launch each per step ----
     hbm, peak_kind = load_peaks()
-    prof = sim_pre.profile()
-    nnz_total = info_pre["nnz_total"]
+    prof = prof_ps if args.no_extras else sim_pre.profile()
     bytes_replay = algorithmic_bytes(n_nodes, M, T, nnz_total)
-    step_launch_ms = prof["step_ms"] / max(1, prof["step_launches"])
+    infect_ms = prof["spmv_ms"] / max(1, prof["spmv_launches"])
+    flow_ms = prof["step_ms"] / max(1, prof["step_launches"])
+    step_launch_ms = infect_ms + flow_ms
     achieved = (bytes_replay / T) / (step_launch_ms / 1e3) / 1e9
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                       "frac": achieved / hbm, "peak_source": peak_kind,
-                       "kernel": "k_packed_step", "algorithmic_bytes_per_launch": bytes_replay / T,
-                       "avg_launch_us": step_launch_ms * 1e3, "traffic": None}
-    prof_ps = sim.profile()
-    out["profile_ms"] = {"prebuilt": prof, "per_step": prof_ps}
+                       "frac": achieved / hbm, "peak_source": f"{peak_kind} (copy bandwidth)",
+                       "kernel": "k_infect + k_flow (the two launches of one step)",
+                       "algorithmic_bytes_per_launch": bytes_replay / T,
+                       "avg_launch_us": step_launch_ms * 1e3,
+                       "avg_launch_us_by_kernel": {"k_infect": infect_ms * 1e3, "k_flow": flow_ms * 1e3},
+                       "traffic": profiled_traffic(args.workload)}
+    out["profile_ms"] = {"per_step": prof} if args.no_extras else {"prebuilt": prof, "per_step": sim.profile()}
 
     if not args.no_extras and rank == 0:
         # ---- plain per-replica SpMV path (drop-in), same workload ----

@@ -225,7 +225,8 @@ struct rp_sim {
       if (!prebuilt && (t == 0 || w != step_win[t - 1])) {
         enqueue_window_build(*g, wsp, w, wins[w], cap, weight_kind,
                              weight_kind == kWeightF32, st);
-        k += 5 + (wins[w].may_truncate ? 1 : 0) + (weight_kind == kWeightF32 ? 2 : 0);
+        // k_hits, k_scan_tiles, k_scan_apply, k_fill (+ k_trunc, + the two row sorts)
+        k += 4 + (wins[w].may_truncate ? 1 : 0) + (weight_kind == kWeightF32 ? 2 : 0);
         mark(kMarkBuild);
       }
       if (path == RP_PATH_PLAIN) {
