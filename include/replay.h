@@ -117,6 +117,26 @@ RP_API rp_status rp_window_csr(rp_graph *g, int64_t ws, int64_t we,
                                int32_t *col, void *val, int64_t capacity,
                                int64_t *nnz, int64_t *n_hits);
 
+/* Allocation-free variant of rp_window_csr, with no counterpart in the
+ * reference: builds the same window CSR on the device and leaves it in
+ * caller-owned device buffers -- d_row_ptr (n_nodes+1 int32) and d_entries
+ * (`capacity` pairs {col, weight} of int32, weight as rp_window_csr's
+ * weight_kind) -- without allocating or freeing device memory.  For callers
+ * that cannot pay cudaFree's device-wide wait per window or that hand all
+ * device memory to their own pool.  Scratch is one static device array
+ * (about 9 MB per device), so the graph may have at most 65,536 nodes and
+ * the window at most 131,072 candidate contacts (RP_ERR_RANGE beyond).
+ * Calls share that scratch: concurrent or overlapping calls race, so issue
+ * them one at a time.  The first call on a device looks the scratch up
+ * (cudaGetSymbolAddress); make it before any stream capture.  Returns when
+ * the CSR is in place; *nnz and *n_hits as for rp_window_csr. */
+RP_API rp_status rp_window_csr_noalloc(rp_graph *g, int64_t ws, int64_t we,
+                                       float scale, int32_t weight_kind,
+                                       int32_t ncls_cap, int32_t *d_row_ptr,
+                                       int32_t *d_entries, int64_t capacity,
+                                       int64_t *nnz, int64_t *n_hits,
+                                       void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* Simulations.                                                              */
 /* ------------------------------------------------------------------------ */

@@ -87,6 +87,9 @@ SIGNATURES = {
     "rp_graph_free": ([C.c_void_p], None),
     "rp_window_csr": ([C.c_void_p, C.c_int64, C.c_int64, C.c_float, C.c_int32, C.c_int32, C.c_void_p,
                        C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
+    "rp_window_csr_noalloc": ([C.c_void_p, C.c_int64, C.c_int64, C.c_float, C.c_int32, C.c_int32, C.c_void_p,
+                               C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_void_p],
+                              C.c_int),
     "rp_params_default": ([C.POINTER(Params)], None),
     "rp_sim_create": ([C.c_void_p, C.POINTER(Params), C.POINTER(C.c_void_p)], C.c_int),
     "rp_sim_free": ([C.c_void_p], None),

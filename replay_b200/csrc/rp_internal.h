@@ -33,6 +33,7 @@ rp_status cuda_fail(cudaError_t e, const char *what);
 struct DevBuf {
   void *ptr = nullptr;
   size_t bytes = 0;
+  bool owned = true;  // false: a view of memory this buffer must not free
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
@@ -51,9 +52,17 @@ struct DevBuf {
     return RP_OK;
   }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr && owned) cudaFree(ptr);
     ptr = nullptr;
     bytes = 0;
+    owned = true;
+  }
+  // Points at memory owned elsewhere (no allocation; release() won't free it).
+  void borrow(void *p, size_t n) {
+    release();
+    ptr = p;
+    bytes = n;
+    owned = false;
   }
   template <typename T>
   T *as() const {
@@ -142,6 +151,9 @@ rp_status window_workspace_alloc(WindowWorkspace &w, int32_t n_nodes,
                                  int64_t cap_hits, int64_t n_windows,
                                  const std::vector<WinDesc> &wins,
                                  const std::vector<CandRange> &ranges);
+
+// Scan tiles the window builder uses for n_nodes rows.
+int32_t window_scan_tiles(int32_t n_nodes);
 
 enum WeightKind { kWeightF32 = 0, kWeightI32 = 1 };
 

@@ -523,6 +523,11 @@ int bits_for(int64_t maxval) {
 
 }  // namespace
 
+int32_t window_scan_tiles(int32_t n_nodes) {
+  const int32_t t = (int32_t)((n_nodes + kScanTile - 1) / kScanTile);
+  return t < 1 ? 1 : t;
+}
+
 rp_status window_workspace_alloc(WindowWorkspace &w, int32_t n_nodes,
                                  int64_t cap_hits, int64_t n_windows,
                                  const std::vector<WinDesc> &wins,
