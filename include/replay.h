@@ -254,6 +254,49 @@ RP_API rp_status rp_sim_profile(rp_sim *s, rp_profile *out);
 RP_API rp_status rp_sim_profile_steps(rp_sim *s, float *step_ms);
 
 /* ------------------------------------------------------------------------ */
+/* Expected-value (mean-field) replay and its adjoint.  No reference        */
+/* counterpart: the differentiable form of the geometric replay.            */
+/* ------------------------------------------------------------------------ */
+typedef struct rp_meanfield rp_meanfield;
+
+/* Builds the schedule and every window CSR (int32 contact-second weights) of
+ * the replay described by p: n_steps, step_size, start_time, window,
+ * ncls_cap, has_exposed and ir_to_s are used; replica and rate fields are
+ * ignored.  The adjoint recomputes states between checkpoints taken every
+ * `checkpoint_every` steps.  The graph must outlive the handle. */
+RP_API rp_status rp_meanfield_create(const rp_graph *g, const rp_params *p,
+                                     int32_t checkpoint_every,
+                                     rp_meanfield **out);
+RP_API void rp_meanfield_free(rp_meanfield *m);
+
+/* Forward replay on device pointers, enqueued on `stream`.  x0: 4*N floats,
+ * the planes S, E, I, R of node probabilities.  Per step, with
+ * e_i = scale * sum_j w_ij I_j and P_i = 1 - exp(-beta s_i e_i):
+ * S' = S(1-P) + p_rs R, E' = E(1-p_ei) + S P, I' = I(1-p_ir) + p_ei E,
+ * R' = R(1-p_rs) + p_ir I (S->I directly without an exposed state; I->S
+ * with ir_to_s).  d_susceptibility: N floats, or NULL for all ones.
+ * d_incidence (n_steps floats): expected new infections sum_i S_i P_i of
+ * each step; d_xT (4*N floats, optional): the final planes.  Keeps the
+ * checkpoints and parameters for rp_meanfield_backward. */
+RP_API rp_status rp_meanfield_forward(rp_meanfield *m, const float *d_x0,
+                                      float beta, const float *d_susceptibility,
+                                      float p_ei, float p_ir, float p_rs,
+                                      float *d_incidence, float *d_xT,
+                                      void *stream);
+
+/* Reverse-time adjoint of the last forward: given dL/dincidence (n_steps
+ * floats, or NULL for zeros) and dL/dx_T (4*N, or NULL), writes dL/dx0
+ * (4*N floats), dL/dsusceptibility (N floats, optional) and d_grad_rates =
+ * dL/d(beta, p_ei, p_ir, p_rs) as 4 doubles on the device (optional; the
+ * scalar reductions run in FP64).  Transpose products use the same CSRs
+ * (window graphs are symmetric). */
+RP_API rp_status rp_meanfield_backward(rp_meanfield *m,
+                                       const float *d_grad_incidence,
+                                       const float *d_grad_xT, float *d_grad_x0,
+                                       float *d_grad_susceptibility,
+                                       double *d_grad_rates, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Kernel test hooks on device pointers.                                     */
 /* ------------------------------------------------------------------------ */
 

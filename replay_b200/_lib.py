@@ -100,6 +100,12 @@ SIGNATURES = {
     "rp_sim_get_info": ([C.c_void_p, C.POINTER(SimInfo)], C.c_int),
     "rp_sim_profile": ([C.c_void_p, C.POINTER(Profile)], C.c_int),
     "rp_sim_profile_steps": ([C.c_void_p, C.c_void_p], C.c_int),
+    "rp_meanfield_create": ([C.c_void_p, C.POINTER(Params), C.c_int32, C.POINTER(C.c_void_p)], C.c_int),
+    "rp_meanfield_free": ([C.c_void_p], None),
+    "rp_meanfield_forward": ([C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_float, C.c_float, C.c_float,
+                              C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "rp_meanfield_backward": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+                               C.c_int),
     "rp_exposure_spmv_f32": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                               C.c_void_p], C.c_int),
     "rp_exposure_spmm_packed": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,

@@ -269,6 +269,22 @@ struct rp_sim {
   }
 };
 
+// Mean-field replay: the schedule and prebuilt window CSRs of a geometric
+// simulation, FP32 probability planes, checkpoints every K steps.
+struct rp_meanfield {
+  rp_sim base;
+  int32_t N = 0, T = 0, K = 24, nblk = 0, n_ckpt = 0;
+  MfRates rates{};
+  bool have_forward = false, has_sus = false;
+  DevBuf ckpt;                 // n_ckpt x 4N: x_0, x_K, x_2K, ...
+  DevBuf xa, xb;               // 4N ping-pong
+  DevBuf seg_x, seg_q, seg_e;  // recomputed segment: K x 4N, K x N, K x N
+  DevBuf inc_part;             // T x blocks incidence partials
+  DevBuf a0, a1, z0, z1;       // adjoint ping-pong (4N), coupling terms (N)
+  DevBuf gpart;                // blocks x 4 FP64 scalar-gradient partials
+  DevBuf sus;                  // copy of the forward's susceptibility
+};
+
 namespace {
 
 // Builds every window's canonical CSR once into the arena.
@@ -893,6 +909,171 @@ RP_API rp_status rp_exposure_spmm_packed(const int32_t *d_row_ptr, const int32_t
   }
   packed_exposure(d_row_ptr, reinterpret_cast<const int2 *>(d_entries), n_nodes, d_masks,
                   words, n_replicas, d_exposure, static_cast<cudaStream_t>(stream));
+  RP_TRY_CUDA(cudaGetLastError());
+  return RP_OK;
+}
+
+// ---- mean-field replay --------------------------------------------------
+
+RP_API rp_status rp_meanfield_create(const rp_graph *h, const rp_params *p,
+                                     int32_t checkpoint_every, rp_meanfield **out) {
+  if (!h || !p || !out) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  if (p->struct_size != sizeof(rp_params)) {
+    set_error("rp_params.struct_size mismatch (%u, expected %zu)", p->struct_size,
+              sizeof(rp_params));
+    return RP_ERR_ARG;
+  }
+  if (checkpoint_every <= 0) {
+    set_error("checkpoint interval must be positive");
+    return RP_ERR_ARG;
+  }
+  *out = nullptr;
+  std::unique_ptr<rp_meanfield> m(new rp_meanfield());
+  rp_params q = *p;
+  q.n_replicas = 32;
+  q.transition = RP_TRANSITION_GEOMETRIC;
+  q.path = RP_PATH_BATCHED;
+  q.csr_mode = RP_CSR_PREBUILT;
+  q.initial_count = 0;
+  q.beta_per_replica = nullptr;
+  q.susceptibility = nullptr;
+  rp_sim &b = m->base;
+  RP_TRY(sim_setup(b, h->g, q));
+  b.prebuilt = true;
+  RP_TRY(prebuild(b));
+  const int32_t N = b.N, T = b.T;
+  m->N = N;
+  m->T = T;
+  m->K = checkpoint_every < (T > 0 ? T : 1) ? checkpoint_every : (T > 0 ? T : 1);
+  m->nblk = mf_blocks(N);
+  m->n_ckpt = T > 0 ? (T + m->K - 1) / m->K : 1;
+  const size_t plane = sizeof(float) * 4 * (size_t)N;
+  RP_TRY(m->ckpt.alloc(plane * m->n_ckpt));
+  RP_TRY(m->xa.alloc(plane));
+  RP_TRY(m->xb.alloc(plane));
+  RP_TRY(m->seg_x.alloc(plane * m->K));
+  RP_TRY(m->seg_q.alloc(sizeof(float) * (size_t)N * m->K));
+  RP_TRY(m->seg_e.alloc(sizeof(float) * (size_t)N * m->K));
+  RP_TRY(m->inc_part.alloc(sizeof(float) * (size_t)m->nblk * (T > 0 ? T : 1)));
+  RP_TRY(m->a0.alloc(plane));
+  RP_TRY(m->a1.alloc(plane));
+  RP_TRY(m->z0.alloc(sizeof(float) * (size_t)N));
+  RP_TRY(m->z1.alloc(sizeof(float) * (size_t)N));
+  RP_TRY(m->gpart.alloc(sizeof(double) * 4 * (size_t)m->nblk));
+  RP_TRY(m->sus.alloc(sizeof(float) * (size_t)N));
+  m->rates.has_exposed = p->has_exposed;
+  m->rates.ir_to_s = p->ir_to_s;
+  *out = m.release();
+  return RP_OK;
+}
+
+RP_API void rp_meanfield_free(rp_meanfield *m) { delete m; }
+
+RP_API rp_status rp_meanfield_forward(rp_meanfield *m, const float *d_x0, float beta,
+                                      const float *d_sus, float p_ei, float p_ir, float p_rs,
+                                      float *d_incidence, float *d_xT, void *stream) {
+  if (!m || !d_x0) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  auto unit = [](float v) { return v >= 0.0f && v <= 1.0f; };
+  if (!(beta >= 0.0f) || !unit(p_ei) || !unit(p_ir) || !unit(p_rs)) {
+    set_error("beta must be >= 0 and the rates in [0, 1]");
+    return RP_ERR_ARG;
+  }
+  RP_TRY_CUDA(cudaSetDevice(m->base.g->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int32_t N = m->N, T = m->T;
+  const size_t plane = sizeof(float) * 4 * (size_t)N;
+  m->rates.beta = beta;
+  m->rates.p_ei = p_ei;
+  m->rates.p_ir = p_ir;
+  m->rates.p_rs = p_rs;
+  m->has_sus = d_sus != nullptr;
+  if (d_sus)
+    RP_TRY_CUDA(cudaMemcpyAsync(m->sus.ptr, d_sus, sizeof(float) * (size_t)N,
+                                cudaMemcpyDeviceToDevice, st));
+  const float *sus = m->has_sus ? m->sus.as<float>() : nullptr;
+  float *ck = m->ckpt.as<float>();
+  RP_TRY_CUDA(cudaMemcpyAsync(ck, d_x0, plane, cudaMemcpyDeviceToDevice, st));
+  const float *cur = ck;
+  float *pp[2] = {m->xa.as<float>(), m->xb.as<float>()};
+  for (int32_t t = 0; t < T; ++t) {
+    float *nxt = pp[t & 1];
+    mf_step(m->base.rp_of(t), m->base.ent_of(t), N, m->base.step_scale[t], m->rates, sus, cur,
+            nxt, nullptr, nullptr, m->inc_part.as<float>() + (size_t)t * m->nblk, st);
+    if ((t + 1) % m->K == 0 && t + 1 < T)
+      RP_TRY_CUDA(cudaMemcpyAsync(ck + (size_t)((t + 1) / m->K) * 4 * N, nxt, plane,
+                                  cudaMemcpyDeviceToDevice, st));
+    cur = nxt;
+  }
+  if (d_incidence) mf_incidence(m->inc_part.as<float>(), m->nblk, T, d_incidence, st);
+  if (d_xT) RP_TRY_CUDA(cudaMemcpyAsync(d_xT, cur, plane, cudaMemcpyDeviceToDevice, st));
+  RP_TRY_CUDA(cudaGetLastError());
+  m->have_forward = true;
+  return RP_OK;
+}
+
+RP_API rp_status rp_meanfield_backward(rp_meanfield *m, const float *d_grad_incidence,
+                                       const float *d_grad_xT, float *d_grad_x0,
+                                       float *d_grad_sus, double *d_grad_rates, void *stream) {
+  if (!m || !d_grad_x0) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  if (!m->have_forward) {
+    set_error("rp_meanfield_backward needs a preceding rp_meanfield_forward");
+    return RP_ERR_ARG;
+  }
+  RP_TRY_CUDA(cudaSetDevice(m->base.g->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int32_t N = m->N, T = m->T, K = m->K;
+  const size_t plane = sizeof(float) * 4 * (size_t)N;
+  const float *sus = m->has_sus ? m->sus.as<float>() : nullptr;
+  const MfRates &r = m->rates;
+  RP_TRY_CUDA(cudaMemsetAsync(m->gpart.ptr, 0, m->gpart.bytes, st));
+  if (d_grad_sus) RP_TRY_CUDA(cudaMemsetAsync(d_grad_sus, 0, sizeof(float) * (size_t)N, st));
+  float *a[2] = {m->a0.as<float>(), m->a1.as<float>()};
+  float *z[2] = {m->z0.as<float>(), m->z1.as<float>()};
+  if (d_grad_xT)
+    RP_TRY_CUDA(cudaMemcpyAsync(a[0], d_grad_xT, plane, cudaMemcpyDeviceToDevice, st));
+  else
+    RP_TRY_CUDA(cudaMemsetAsync(a[0], 0, plane, st));
+  int ai = 0;
+  const float *ck = m->ckpt.as<float>();
+  float *sx = m->seg_x.as<float>(), *sq = m->seg_q.as<float>(), *se = m->seg_e.as<float>();
+  // x of step t within the recomputed segment starting at c0
+  auto seg_state = [&](int32_t c0, int32_t t) -> const float * {
+    return t == c0 ? ck + (size_t)(c0 / K) * 4 * N : sx + (size_t)(t - c0) * 4 * N;
+  };
+  for (int32_t t = T - 1; t >= 0; --t) {
+    const int32_t c0 = (t / K) * K;
+    if (t == T - 1 || t == c0 + K - 1) {
+      // recompute the segment [c0, t]: states, exp(-beta s e) and scaled exposures
+      for (int32_t u = c0; u <= t; ++u) {
+        float *xo = u + 1 <= t ? sx + (size_t)(u + 1 - c0) * 4 * N : m->xa.as<float>();
+        mf_step(m->base.rp_of(u), m->base.ent_of(u), N, m->base.step_scale[u], r, sus,
+                seg_state(c0, u), xo, sq + (size_t)(u - c0) * N, se + (size_t)(u - c0) * N,
+                m->inc_part.as<float>() + (size_t)u * m->nblk, st);
+      }
+    }
+    const bool couple = t + 1 < T;
+    mf_adjoint(N, couple ? m->base.rp_of(t + 1) : nullptr,
+               couple ? m->base.ent_of(t + 1) : nullptr, z[(t + 1) & 1], a[ai],
+               seg_state(c0, t), sq + (size_t)(t - c0) * N, se + (size_t)(t - c0) * N,
+               d_grad_incidence, t, m->base.step_scale[t], r, sus, a[ai ^ 1], z[t & 1],
+               d_grad_sus, m->gpart.as<double>(), st);
+    ai ^= 1;
+  }
+  if (T > 0)
+    mf_adjoint(N, m->base.rp_of(0), m->base.ent_of(0), z[0], a[ai], nullptr, nullptr, nullptr,
+               nullptr, 0, 1.0f, r, sus, d_grad_x0, nullptr, nullptr, nullptr, st);
+  else
+    RP_TRY_CUDA(cudaMemcpyAsync(d_grad_x0, a[ai], plane, cudaMemcpyDeviceToDevice, st));
+  if (d_grad_rates) mf_finish(m->gpart.as<double>(), m->nblk, d_grad_rates, st);
   RP_TRY_CUDA(cudaGetLastError());
   return RP_OK;
 }

@@ -1,0 +1,128 @@
+"""Differentiable expected-value (mean-field) replay as a torch op.
+
+`MeanField(graph, iterations=..., ...)` holds the schedule and every window
+CSR of a replay on the graph's GPU (rp_meanfield_create).  Calling it runs
+the forward kernels on the current torch stream and returns
+
+    incidence  (iterations,)  expected new infections per step
+    x_T        (4, N)         final S, E, I, R probabilities
+
+as tensors of a torch.autograd.Function whose backward is the hand-written
+reverse-time adjoint (rp_meanfield_backward): gradients flow to x0, beta,
+the per-node susceptibility and the E->I, I->R, R->S rates.
+
+    mf = MeanField(g, iterations=336, step_size=3600, window=3600, start_time=t0)
+    inc, xT = mf(x0, beta, susceptibility=s, p_ei=1/48, p_ir=1/120)
+    loss = ((inc.view(-1, 24).sum(1) - target) ** 2).mean()
+    loss.backward()
+
+Everything runs on the GPU through libreplay; there is no CPU path.
+"""
+import ctypes as C
+
+import torch
+
+from . import _lib
+from ._lib import check, lib
+
+__all__ = ["MeanField"]
+
+
+def _scalar(v, like):
+    if isinstance(v, torch.Tensor):
+        return v
+    return torch.tensor(float(v), dtype=torch.float32, device=like.device)
+
+
+class _MeanFieldFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, mf, x0, beta, sus, p_ei, p_ir, p_rs):
+        x0c = x0.detach().to(torch.float32).contiguous()
+        susc = sus.detach().to(torch.float32).contiguous() if sus is not None else None
+        rates = [float(v) for v in (beta, p_ei, p_ir, p_rs)]
+        inc, xT = mf._forward(x0c, susc, rates)
+        ctx.mf = mf
+        ctx.generation = mf._generation
+        ctx.inputs = (x0c, susc, rates)
+        ctx.has_sus = sus is not None
+        ctx.rate_dtypes = [getattr(v, "dtype", torch.float32) for v in (beta, p_ei, p_ir, p_rs)]
+        return inc, xT
+
+    @staticmethod
+    def backward(ctx, g_inc, g_xT):
+        mf = ctx.mf
+        if mf._generation != ctx.generation:  # another forward ran since: restore its checkpoints
+            mf._forward(*ctx.inputs)
+        dev = mf.device
+        g_inc = g_inc.to(torch.float32).contiguous() if g_inc is not None else None
+        g_xT = g_xT.to(torch.float32).contiguous() if g_xT is not None else None
+        gx0 = torch.empty((4, mf.N), dtype=torch.float32, device=dev)
+        gsus = torch.empty(mf.N, dtype=torch.float32, device=dev) if ctx.has_sus else None
+        grates = torch.empty(4, dtype=torch.float64, device=dev)
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+        check(lib().rp_meanfield_backward(mf._h, ptr(g_inc), ptr(g_xT), ptr(gx0), ptr(gsus), ptr(grates),
+                                          C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+        g = [grates[k].to(ctx.rate_dtypes[k]) for k in range(4)]
+        return None, gx0, g[0], gsus, g[1], g[2], g[3]
+
+
+class MeanField:
+    """Expected-value replay over a Graph's per-step window CSRs.
+
+    Keyword arguments follow Simulation: iterations (n_steps), step_size,
+    start_time, window, has_exposed, ir_to_s, ncls_cap; checkpoint_every is
+    the adjoint's checkpoint interval in steps (states in between are
+    recomputed)."""
+
+    _ALIASES = {"iterations": "n_steps", "static_network_duration": "window"}
+
+    def __init__(self, graph, checkpoint_every=24, **kw):
+        p = _lib.Params()
+        lib().rp_params_default(C.byref(p))
+        for k, val in kw.items():
+            k = self._ALIASES.get(k, k)
+            if k in ("ncls_cap", "has_exposed", "ir_to_s"):
+                val = int(bool(val))
+            if k not in ("n_steps", "step_size", "start_time", "window", "ncls_cap", "has_exposed", "ir_to_s"):
+                raise TypeError(f"unknown mean-field parameter {k!r}")
+            setattr(p, k, val)
+        self.graph = graph
+        self.N = graph.n_nodes
+        self.T = p.n_steps
+        self.device = torch.device("cuda", graph.info["device"])
+        h = C.c_void_p()
+        check(lib().rp_meanfield_create(graph._h, C.byref(p), int(checkpoint_every), C.byref(h)))
+        self._h = h
+        self._generation = 0
+
+    def _forward(self, x0, sus, rates):
+        if x0.shape != (4, self.N) or x0.device != self.device:
+            raise ValueError(f"x0 must be a (4, {self.N}) tensor on {self.device}")
+        if sus is not None and (sus.shape != (self.N,) or sus.device != self.device):
+            raise ValueError(f"susceptibility must be a ({self.N},) tensor on {self.device}")
+        inc = torch.empty(self.T, dtype=torch.float32, device=self.device)
+        xT = torch.empty((4, self.N), dtype=torch.float32, device=self.device)
+        beta, p_ei, p_ir, p_rs = rates
+        check(lib().rp_meanfield_forward(
+            self._h, C.c_void_p(x0.data_ptr()), beta, C.c_void_p(sus.data_ptr()) if sus is not None else None,
+            p_ei, p_ir, p_rs, C.c_void_p(inc.data_ptr()), C.c_void_p(xT.data_ptr()),
+            C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)))
+        self._generation += 1
+        return inc, xT
+
+    def __call__(self, x0, beta, susceptibility=None, p_ei=0.0, p_ir=0.0, p_rs=0.0):
+        x0 = x0.reshape(4, self.N)
+        beta = _scalar(beta, x0)
+        p_ei, p_ir, p_rs = (_scalar(v, x0) for v in (p_ei, p_ir, p_rs))
+        return _MeanFieldFn.apply(self, x0, beta, susceptibility, p_ei, p_ir, p_rs)
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().rp_meanfield_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,156 @@
+"""Mean-field (expected-value) replay: the FP32 forward and adjoint kernels
+against a float64 torch reference on the oracle's window CSRs, and against
+float64 central finite differences.  The reference itself is pinned on the
+CPU (autograd vs finite differences, conservation)."""
+import numpy as np
+import pytest
+import torch
+
+from replay_b200 import synthetic
+
+STEP = dict(step_size=3600.0, window=3600)
+
+
+def _net(seed=50, n_nodes=160, n_contacts=5000):
+    return synthetic.tiny(seed=seed, n_nodes=n_nodes, n_contacts=n_contacts, span=40 * 3600, max_dur=3000)
+
+
+def _x0(n, seed=0):
+    g = torch.Generator().manual_seed(seed)
+    inf = (torch.rand(n, generator=g, dtype=torch.float64) < 0.08).double() * 0.9
+    x0 = torch.zeros(4, n, dtype=torch.float64)
+    x0[2] = inf
+    x0[0] = 1 - inf
+    return x0
+
+
+def _csrs(net, T, **kw):
+    from oracle import meanfield_ref
+    return meanfield_ref.window_csrs(net["start"], net["end"], net["u"], net["v"], net["n_nodes"], net["t0"],
+                                     STEP["step_size"], kw.get("window", STEP["window"]), T)
+
+
+def test_reference_autograd_matches_finite_differences():
+    from oracle import meanfield_ref as mr
+    net = _net(n_nodes=60, n_contacts=1500)
+    T = 30
+    csrs = _csrs(net, T)
+    n = net["n_nodes"]
+    x0 = _x0(n)
+    sus = torch.linspace(0.5, 1.5, n, dtype=torch.float64)
+    c = torch.linspace(-1, 1, T, dtype=torch.float64)
+    base = dict(beta=2e-4, p_ei=0.2, p_ir=0.1, p_rs=0.05)
+
+    def loss(**kw):
+        args = dict(base, **kw)
+        inc, xT = mr.forward(csrs, x0, args["beta"], sus, args["p_ei"], args["p_ir"], args["p_rs"])
+        return (c * inc).sum() + xT[2].sum() * 0.3
+
+    params = {k: torch.tensor(v, dtype=torch.float64, requires_grad=True) for k, v in base.items()}
+    L = loss(**params)
+    L.backward()
+    for k, v in base.items():
+        fd = mr.central_difference(lambda h, k=k: loss(**{k: h}), v)
+        assert abs(params[k].grad.item() - fd) <= 1e-6 * max(abs(fd), 1e-3), k
+    inc, xT = mr.forward(csrs, x0, base["beta"], sus, base["p_ei"], base["p_ir"], base["p_rs"])
+    torch.testing.assert_close(xT.sum(0), x0.sum(0))
+
+
+def _loss_weights(T, n, seed=3):
+    g = torch.Generator().manual_seed(seed)
+    return torch.rand(T, generator=g, dtype=torch.float64) - 0.5, torch.rand(4, n, generator=g,
+                                                                            dtype=torch.float64) - 0.5
+
+
+VARIANTS = [dict(has_exposed=True, ir_to_s=False, p_rs=0.05),
+            dict(has_exposed=False, ir_to_s=False, p_rs=0.0),
+            dict(has_exposed=False, ir_to_s=True, p_rs=0.0)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", range(len(VARIANTS)))
+@pytest.mark.parametrize("checkpoint_every", [1, 7, 48])
+def test_gpu_forward_and_adjoint_match_float64_reference(variant, checkpoint_every):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import replay_b200 as rb
+    from oracle import meanfield_ref as mr
+    from replay_b200.meanfield import MeanField
+    v = VARIANTS[variant]
+    net = _net()
+    n, T = net["n_nodes"], 48
+    g = rb.Graph.from_arrays(net["start"], net["end"], net["u"], net["v"], n)
+    mf = MeanField(g, iterations=T, start_time=net["t0"], has_exposed=v["has_exposed"], ir_to_s=v["ir_to_s"],
+                   checkpoint_every=checkpoint_every, **STEP)
+    x0 = _x0(n)
+    sus = torch.linspace(0.5, 1.5, n, dtype=torch.float64)
+    rates = dict(beta=1.5e-4, p_ei=0.25, p_ir=0.12, p_rs=v["p_rs"])
+    c, d = _loss_weights(T, n)
+
+    # float64 reference with autograd
+    rp = {k: torch.tensor(val, dtype=torch.float64, requires_grad=True) for k, val in rates.items()}
+    x0r = x0.clone().requires_grad_(True)
+    susr = sus.clone().requires_grad_(True)
+    inc_r, xT_r = mr.forward(_csrs(net, T), x0r, rp["beta"], susr, rp["p_ei"], rp["p_ir"], rp["p_rs"],
+                             has_exposed=v["has_exposed"], ir_to_s=v["ir_to_s"])
+    Lr = (c * inc_r).sum() + (d * xT_r).sum()
+    Lr.backward()
+
+    # FP32 kernels
+    dev = torch.device("cuda")
+    gp = {k: torch.tensor(val, dtype=torch.float32, device=dev, requires_grad=True) for k, val in rates.items()}
+    x0g = x0.float().to(dev).requires_grad_(True)
+    susg = sus.float().to(dev).requires_grad_(True)
+    inc, xT = mf(x0g, gp["beta"], susceptibility=susg, p_ei=gp["p_ei"], p_ir=gp["p_ir"], p_rs=gp["p_rs"])
+    L = (c.float().to(dev) * inc).sum() + (d.float().to(dev) * xT).sum()
+    L.backward()
+
+    torch.testing.assert_close(inc.double().cpu(), inc_r.detach(), rtol=2e-5, atol=1e-5)
+    torch.testing.assert_close(xT.double().cpu(), xT_r.detach(), rtol=2e-5, atol=2e-6)
+    for k in rates:
+        got = gp[k].grad.item()
+        if rp[k].grad is None:  # parameter unused in this variant (p_ei without an exposed state)
+            assert got == 0.0, k
+            continue
+        want = rp[k].grad.item()
+        assert abs(got - want) <= 1e-4 * abs(want) + 1e-7, (k, got, want)
+    for got, want in ((susg.grad, susr.grad), (x0g.grad, x0r.grad)):
+        err = (got.double().cpu() - want).norm() / want.norm()
+        assert err <= 1e-4, err.item()
+
+
+@pytest.mark.gpu
+def test_gpu_adjoint_matches_finite_differences_and_repeats():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import replay_b200 as rb
+    from oracle import meanfield_ref as mr
+    from replay_b200.meanfield import MeanField
+    net = _net(seed=51)
+    n, T = net["n_nodes"], 48
+    g = rb.Graph.from_arrays(net["start"], net["end"], net["u"], net["v"], n)
+    mf = MeanField(g, iterations=T, start_time=net["t0"], checkpoint_every=12, **STEP)
+    csrs = _csrs(net, T)
+    x0 = _x0(n, seed=1)
+    sus = torch.linspace(0.6, 1.4, n, dtype=torch.float64)
+    target = torch.linspace(0.5, 3.0, T // 24, dtype=torch.float64)
+    base = dict(beta=1e-4, p_ei=0.2, p_ir=0.1)
+
+    def ref_loss(**kw):
+        a = dict(base, **kw)
+        inc, _ = mr.forward(csrs, x0, a["beta"], sus, a["p_ei"], a["p_ir"], 0.0)
+        return ((inc.view(-1, 24).sum(1) - target) ** 2).mean()
+
+    dev = torch.device("cuda")
+    grads = []
+    for _ in range(2):  # two backward passes in a row give identical gradients
+        gp = {k: torch.tensor(v, dtype=torch.float32, device=dev, requires_grad=True) for k, v in base.items()}
+        inc, _ = mf(x0.float().to(dev), gp["beta"], susceptibility=sus.float().to(dev), p_ei=gp["p_ei"],
+                    p_ir=gp["p_ir"])
+        L = ((inc.view(-1, 24).sum(1) - target.float().to(dev)) ** 2).mean()
+        L.backward()
+        grads.append({k: gp[k].grad.item() for k in base})
+    assert grads[0] == grads[1]
+    for k, v in base.items():
+        fd = mr.central_difference(lambda h, k=k: ref_loss(**{k: h}), v)
+        assert abs(grads[0][k] - fd) <= 1e-4 * abs(fd), (k, grads[0][k], fd)
