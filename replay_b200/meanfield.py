@@ -19,13 +19,14 @@ the per-node susceptibility and the E->I, I->R, R->S rates.
 Everything runs on the GPU through libreplay; there is no CPU path.
 """
 import ctypes as C
+import math
 
 import torch
 
 from . import _lib
 from ._lib import check, lib
 
-__all__ = ["MeanField"]
+__all__ = ["MeanField", "daily_incidence", "calibrate_beta"]
 
 
 def _scalar(v, like):
@@ -126,3 +127,30 @@ class MeanField:
             self.close()
         except Exception:
             pass
+
+
+def daily_incidence(incidence, steps_per_day):
+    """Sums per-step incidence into days (trailing partial day dropped)."""
+    days = incidence.shape[-1] // steps_per_day
+    return incidence[..., :days * steps_per_day].reshape(*incidence.shape[:-1], days, steps_per_day).sum(-1)
+
+
+def calibrate_beta(mf, x0, target_daily, beta0, steps_per_day=24, susceptibility=None, p_ei=0.0, p_ir=0.0,
+                   p_rs=0.0, iters=60, lr=0.1):
+    """Fits the global transmission rate beta so that the mean-field daily
+    incidence matches `target_daily` in mean squared error (Adam on log beta,
+    gradients from the adjoint).  Returns (beta, per-iteration losses)."""
+    dev = mf.device
+    target = torch.as_tensor(target_daily, dtype=torch.float32, device=dev)
+    x0 = torch.as_tensor(x0, dtype=torch.float32, device=dev)
+    logb = torch.tensor(math.log(beta0), dtype=torch.float32, device=dev, requires_grad=True)
+    opt = torch.optim.Adam([logb], lr=lr)
+    losses = []
+    for _ in range(iters):
+        opt.zero_grad()
+        inc, _ = mf(x0, logb.exp(), susceptibility=susceptibility, p_ei=p_ei, p_ir=p_ir, p_rs=p_rs)
+        loss = ((daily_incidence(inc, steps_per_day) - target) ** 2).mean()
+        loss.backward()
+        opt.step()
+        losses.append(float(loss.detach()))
+    return float(logb.detach().exp()), losses

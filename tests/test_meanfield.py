@@ -154,3 +154,44 @@ def test_gpu_adjoint_matches_finite_differences_and_repeats():
     for k, v in base.items():
         fd = mr.central_difference(lambda h, k=k: ref_loss(**{k: h}), v)
         assert abs(grads[0][k] - fd) <= 1e-4 * abs(fd), (k, grads[0][k], fd)
+
+
+def _mc_daily(rb, g, p, beta, seed, sus):
+    """Mean daily incidence over the Monte Carlo replicas (no waning: new
+    infections of a day = susceptibles lost)."""
+    sim = rb.Simulation(g, path="batched", **dict(p, beta=beta, seed=seed, susceptibility=sus))
+    counts = sim.run()
+    S = counts[:, :, 3].astype(np.float64).mean(axis=1)  # (T+1,)
+    new = S[:-1] - S[1:]
+    return new.reshape(-1, 24).sum(1)
+
+
+@pytest.mark.gpu
+def test_calibrated_beta_reproduces_monte_carlo_incidence():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import replay_b200 as rb
+    from replay_b200.meanfield import MeanField, calibrate_beta
+    net = synthetic.small_seir(seed=7)
+    n, T = net["n_nodes"], 168
+    g = rb.Graph.from_arrays(net["start"], net["end"], net["u"], net["v"], n)
+    sus = np.random.default_rng(0).uniform(0.5, 1.5, n).astype(np.float32)
+    p = dict(M=2048, iterations=T, step_size=3600.0, window=3600, start_time=net["params"]["start_time"],
+             transition="geometric", p_ei=1 / 48, p_ir=1 / 120, initial_count=10)
+    beta_true, beta0 = 6e-5, 2e-5
+    target = _mc_daily(rb, g, p, beta_true, 1, sus)
+    mf = MeanField(g, iterations=T, step_size=3600.0, window=3600, start_time=p["start_time"])
+    x0 = torch.zeros(4, n)
+    x0[2] = 10.0 / n
+    x0[0] = 1 - 10.0 / n
+    beta_cal, losses = calibrate_beta(mf, x0, target, beta0, susceptibility=torch.from_numpy(sus).cuda(),
+                                      p_ei=1 / 48, p_ir=1 / 120, iters=80, lr=0.08)
+    print(f"beta_cal {beta_cal:.3e} loss {losses[0]:.3f} -> {losses[-1]:.3f}")
+    assert losses[-1] < 0.2 * losses[0]
+    assert beta_true / 2.5 < beta_cal < beta_true * 2.5
+    # the Monte Carlo judges: at the calibrated beta it reproduces the target
+    # curve far better than at the starting value
+    judge = lambda b: float(((_mc_daily(rb, g, p, b, 2, sus) - target) ** 2).mean())  # noqa: E731
+    j_cal, j0 = judge(beta_cal), judge(beta0)
+    print(f"MC judge: calibrated {j_cal:.3f} start {j0:.3f}")
+    assert j_cal < 0.25 * j0
