@@ -195,6 +195,18 @@ RP_API void rp_params_default(rp_params *p);
  * set-up in tool/gpu_cpu_temporal_sim.cu:753-857. */
 RP_API rp_status rp_sim_create(const rp_graph *g, const rp_params *p,
                                rp_sim **out);
+/* Independent networks of uneven size batched into one replay (no
+ * reference counterpart; the reference runs one network per process).  The
+ * graph holds the union of the networks, network k owning the nodes
+ * [net_first[k], net_first[k+1]) (n_networks+1 offsets, from 0 to the
+ * graph's n_nodes); contacts between networks would couple them.  All
+ * networks share the schedule and every parameter; initial_count applies to
+ * each (network, replica).  Counts are (n_steps+1) x n_networks x
+ * n_replicas x 4.  Batched (geometric) path only, with ncls_cap = 0: the
+ * reference's hit cap is a property of one network's own index. */
+RP_API rp_status rp_sim_create_batch(const rp_graph *g, const rp_params *p,
+                                     const int32_t *net_first,
+                                     int32_t n_networks, rp_sim **out);
 RP_API void rp_sim_free(rp_sim *s);
 
 /* Per-step node states: states[r * n_nodes + i] in {0 susceptible,

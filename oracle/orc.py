@@ -37,6 +37,8 @@ class Params(C.Structure):
         ("has_exposed", C.c_int32),
         ("ir_to_s", C.c_int32),
         ("ncls_cap", C.c_int32),
+        ("net_first", C.c_void_p),
+        ("n_nets", C.c_int32),
     ]
 
 
@@ -228,7 +230,7 @@ def run(start, end, u, v, n_nodes, node_states=False, **kw):
                     p_rs=0.0, has_exposed=1, ir_to_s=0, ncls_cap=1)
     keep = []
     for k, val in {**defaults, **kw}.items():
-        if k in ("beta_per_replica", "susceptibility"):
+        if k in ("beta_per_replica", "susceptibility", "net_first"):
             continue
         setattr(p, k, val)
     for k in ("beta_per_replica", "susceptibility"):
@@ -236,15 +238,22 @@ def run(start, end, u, v, n_nodes, node_states=False, **kw):
             arr = np.ascontiguousarray(kw[k], np.float32)
             keep.append(arr)
             setattr(p, k, arr.ctypes.data)
+    n_nets = 1
+    if kw.get("net_first") is not None:
+        nf = np.ascontiguousarray(kw["net_first"], np.int32)
+        keep.append(nf)
+        n_nets = len(nf) - 1
+        p.net_first, p.n_nets = nf.ctypes.data, n_nets
     T, M = p.n_steps, p.n_replicas
-    counts = np.zeros((T + 1) * M * 4, np.int32)
+    counts = np.zeros((T + 1) * n_nets * M * 4, np.int32)
     ns = np.zeros((T + 1) * M * n_nodes, np.uint8) if node_states else None
     rc = lib().orc_run(np.ascontiguousarray(start, np.int64), np.ascontiguousarray(end, np.int64),
                        np.ascontiguousarray(u, np.int32), np.ascontiguousarray(v, np.int32), len(start),
                        n_nodes, C.byref(p), counts, ns.ctypes.data if ns is not None else None)
     if rc:
         raise RuntimeError(f"orc_run failed ({rc})")
-    counts = counts.reshape(T + 1, M, 4)
+    counts = counts.reshape(T + 1, n_nets, M, 4) if n_nets > 1 or kw.get("net_first") is not None \
+        else counts.reshape(T + 1, M, 4)
     if node_states:
         return counts, ns.reshape(T + 1, M, n_nodes)
     return counts

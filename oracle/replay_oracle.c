@@ -741,13 +741,14 @@ int orc_countdown_class(int32_t c, int32_t E, int32_t I, int32_t R) {
   return 0;
 }
 
-/* Floyd's algorithm: k distinct nodes out of n for replica r. */
-static void exact_k(uint64_t seed, uint32_t r, int32_t n, int32_t k,
+/* Floyd's algorithm: k distinct nodes out of n for replica r of network
+ * `net` (node indices within the network; stream 2 + 4 net). */
+static void exact_k(uint64_t seed, uint32_t r, uint32_t net, int32_t n, int32_t k,
                     int32_t *chosen) {
   uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
   int32_t cnt = 0;
   for (int32_t j = n - k; j < n; j++) {
-    uint32_t ctr[4] = {(uint32_t)j, 0xFFFFFFFEu, r, 2u};
+    uint32_t ctr[4] = {(uint32_t)j, 0xFFFFFFFEu, r, 2u + 4u * net};
     uint32_t out[4];
     orc_philox4x32_10(ctr, key, out);
     uint64_t r64 = (uint64_t)out[0] | ((uint64_t)out[1] << 32);
@@ -820,16 +821,21 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
   const uint64_t ti = orc_threshold64(p->p_ir, &ti_all);
   const uint64_t tr = orc_threshold64(p->p_rs, &tr_all);
 
+  /* network partition (one network spanning all nodes without a batch) */
+  const int32_t n_nets = p->net_first ? p->n_nets : 1;
+  int32_t one_net[2] = {0, N};
+  const int32_t *nf = p->net_first ? p->net_first : one_net;
   /* initial state */
-  if (p->initial_count > 0 && p->initial_count > N) {
-    return 3;
-  }
+  for (int32_t k = 0; k < n_nets; k++)
+    if (p->initial_count > 0 && p->initial_count > nf[k + 1] - nf[k]) return 3;
   for (int32_t r = 0; r < M; r++) {
     if (p->initial_count > 0) {
-      exact_k(p->seed, (uint32_t)r, N, p->initial_count, chosen);
-      for (int32_t q = 0; q < p->initial_count; q++) {
-        int64_t idx = chosen[q] + (int64_t)r * N;
-        cd[idx] = countdown ? (int32_t)((float)medium + p->step_size) : 2;
+      for (int32_t k = 0; k < n_nets; k++) {
+        exact_k(p->seed, (uint32_t)r, (uint32_t)k, nf[k + 1] - nf[k], p->initial_count, chosen);
+        for (int32_t q = 0; q < p->initial_count; q++) {
+          int64_t idx = nf[k] + chosen[q] + (int64_t)r * N;
+          cd[idx] = countdown ? (int32_t)((float)medium + p->step_size) : 2;
+        }
       }
     } else {
       for (int32_t i = 0; i < N; i++) {
@@ -842,21 +848,22 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
 
 #define ORC_RECORD(tidx)                                                      \
   do {                                                                        \
-    for (int32_t r = 0; r < M; r++) {                                         \
-      int32_t cnt4[4] = {0, 0, 0, 0};                                         \
-      for (int32_t i = 0; i < N; i++) {                                       \
-        int32_t c = cd[i + (int64_t)r * N];                                   \
-        int cls = countdown ? orc_countdown_class(c, Ed, Id, Rd) : c;         \
-        cnt4[cls]++;                                                          \
-        if (node_states)                                                      \
-          node_states[((int64_t)(tidx) * M + r) * N + i] = (uint8_t)cls;      \
+    for (int32_t k = 0; k < n_nets; k++)                                      \
+      for (int32_t r = 0; r < M; r++) {                                       \
+        int32_t cnt4[4] = {0, 0, 0, 0};                                       \
+        for (int32_t i = nf[k]; i < nf[k + 1]; i++) {                         \
+          int32_t c = cd[i + (int64_t)r * N];                                 \
+          int cls = countdown ? orc_countdown_class(c, Ed, Id, Rd) : c;       \
+          cnt4[cls]++;                                                        \
+          if (node_states)                                                    \
+            node_states[((int64_t)(tidx) * M + r) * N + i] = (uint8_t)cls;    \
+        }                                                                     \
+        int32_t *row = counts + (((int64_t)(tidx) * n_nets + k) * M + r) * 4; \
+        row[0] = cnt4[1];                                                     \
+        row[1] = cnt4[2];                                                     \
+        row[2] = cnt4[3];                                                     \
+        row[3] = cnt4[0];                                                     \
       }                                                                       \
-      int32_t *row = counts + ((int64_t)(tidx) * M + r) * 4;                  \
-      row[0] = cnt4[1];                                                       \
-      row[1] = cnt4[2];                                                       \
-      row[2] = cnt4[3];                                                       \
-      row[3] = cnt4[0];                                                       \
-    }                                                                         \
   } while (0)
 
   ORC_RECORD(0);

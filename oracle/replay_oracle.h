@@ -128,9 +128,14 @@ typedef struct {
   int32_t has_exposed; /* 0: S->I directly */
   int32_t ir_to_s;     /* 1: I->S (SIS) */
   int32_t ncls_cap;    /* 1: apply the reference's hit cap */
+  /* optional batch of independent networks: network k owns the nodes
+   * [net_first[k], net_first[k+1]); counts become per (network, replica) */
+  const int32_t *net_first; /* n_nets + 1 offsets, or NULL for one network */
+  int32_t n_nets;
 } orc_params;
 
-/* Runs the whole replay.  counts: (n_steps+1) x n_replicas x 4 int32 rows of
+/* Runs the whole replay.  counts: (n_steps+1) x n_nets x n_replicas x 4
+ * int32 rows (n_nets = 1 without a batch) of
  * (exposed, infectious, resistant, susceptible); row 0 is the initial state.
  * Optional node_states: (n_steps+1) x n_replicas x n_nodes uint8 of
  * 0 susceptible, 1 exposed/incubating, 2 infectious, 3 resistant.

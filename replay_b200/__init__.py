@@ -22,7 +22,8 @@ import numpy as np
 from . import _lib
 from ._lib import CLI_PATH, ReplayError, check, lib
 
-__all__ = ["Graph", "Simulation", "ReplayError", "window_csr", "parse_contacts", "CLI_PATH", "version"]
+__all__ = ["Graph", "Simulation", "ReplayError", "window_csr", "parse_contacts", "batch_networks", "CLI_PATH",
+           "version"]
 
 
 def version():
@@ -106,6 +107,22 @@ class Graph:
             pass
 
 
+def batch_networks(networks):
+    """Concatenates independent networks (dicts with start, end, u, v,
+    n_nodes) into one union contact list; returns (start, end, u, v,
+    n_nodes, offsets) with network k's nodes at [offsets[k], offsets[k+1])."""
+    offsets = np.zeros(len(networks) + 1, np.int64)
+    for k, net in enumerate(networks):
+        offsets[k + 1] = offsets[k] + int(net["n_nodes"])
+    if offsets[-1] >= 2 ** 31:
+        raise ValueError("the batch exceeds 2^31 nodes")
+    start = np.concatenate([np.asarray(n["start"], np.int64) for n in networks])
+    end = np.concatenate([np.asarray(n["end"], np.int64) for n in networks])
+    u = np.concatenate([np.asarray(n["u"], np.int64) + offsets[k] for k, n in enumerate(networks)]).astype(np.int32)
+    v = np.concatenate([np.asarray(n["v"], np.int64) + offsets[k] for k, n in enumerate(networks)]).astype(np.int32)
+    return start, end, u, v, int(offsets[-1]), offsets.astype(np.int32)
+
+
 def window_csr(graph, ws, we, scale=1.0, weight="f32", ncls_cap=True):
     """Canonical symmetric CSR of window [ws, we) built on the GPU.
 
@@ -140,16 +157,22 @@ class Simulation:
       infect_prob, initial_infected, initial_count, beta, beta_per_replica,
       susceptibility, p_ei, p_ir, p_rs, has_exposed, ir_to_s, ncls_cap,
       record_node_states.
+    networks: optional node offsets (n_networks + 1) of independent networks
+      batched in the graph (see batch_networks); counts then carry a network
+      axis, (T+1, n_networks, M, 4).  A batch runs on the batched path with
+      the hit cap off (ncls_cap defaults to False).
     """
 
     _ALIASES = {"M": "n_replicas", "iterations": "n_steps", "static_network_duration": "window",
                 "time_step": "window"}
 
-    def __init__(self, graph, **kw):
+    def __init__(self, graph, networks=None, **kw):
         self.graph = graph
         p = _lib.Params()
         lib().rp_params_default(C.byref(p))
         self._keep = []
+        if networks is not None:
+            kw.setdefault("ncls_cap", False)
         for k, val in kw.items():
             k = self._ALIASES.get(k, k)
             if k == "transition":
@@ -171,9 +194,24 @@ class Simulation:
             setattr(p, k, val)
         self.params = p
         h = C.c_void_p()
-        check(lib().rp_sim_create(graph._h, C.byref(p), C.byref(h)))
+        if networks is None:
+            self.n_networks = None
+            check(lib().rp_sim_create(graph._h, C.byref(p), C.byref(h)))
+        else:
+            nf = np.ascontiguousarray(networks, np.int32)
+            self._keep.append(nf)
+            self.n_networks = len(nf) - 1
+            check(lib().rp_sim_create_batch(graph._h, C.byref(p), _ptr(nf), self.n_networks, C.byref(h)))
         self._h = h
         self.M, self.T = p.n_replicas, p.n_steps
+
+    def _shape(self, flat):
+        if self.n_networks is None:
+            return flat.reshape(self.T + 1, self.M, 4)
+        return flat.reshape(self.T + 1, self.n_networks, self.M, 4)
+
+    def _zeros(self):
+        return np.zeros((self.T + 1) * (self.n_networks or 1) * self.M * 4, np.int32)
 
     @property
     def info(self):
@@ -182,11 +220,12 @@ class Simulation:
         return {k: getattr(si, k) for k, _ in si._fields_}
 
     def run(self, node_states=None):
-        """Runs the replay; returns counts (T+1, M, 4) as (E, I, R, S).
+        """Runs the replay; returns counts (T+1, M, 4) as (E, I, R, S)
+        ((T+1, n_networks, M, 4) for a network batch).
 
         node_states: optional callable(step_index, timestamp, states[M, N])
         (requires record_node_states=True)."""
-        counts = np.zeros((self.T + 1) * self.M * 4, np.int32)
+        counts = self._zeros()
         if node_states is not None:
             def _cb(user, step_index, ts, states, n, m):
                 arr = np.ctypeslib.as_array(states, shape=(m * n,)).reshape(m, n).copy()
@@ -195,7 +234,7 @@ class Simulation:
         else:
             cb = _lib.STATE_CB()
         check(lib().rp_sim_run(self._h, _ptr(counts), cb, None))
-        return counts.reshape(self.T + 1, self.M, 4)
+        return self._shape(counts)
 
     def profile(self):
         """Device time per kernel group of one eager replay (CUDA events)."""
@@ -214,9 +253,9 @@ class Simulation:
         check(lib().rp_sim_enqueue(self._h, C.c_void_p(stream) if stream else None))
 
     def counts(self):
-        counts = np.zeros((self.T + 1) * self.M * 4, np.int32)
+        counts = self._zeros()
         check(lib().rp_sim_counts(self._h, _ptr(counts)))
-        return counts.reshape(self.T + 1, self.M, 4)
+        return self._shape(counts)
 
     def timestamps(self):
         ts = np.zeros(self.T + 1, np.int64)

@@ -92,6 +92,8 @@ SIGNATURES = {
                               C.c_int),
     "rp_params_default": ([C.POINTER(Params)], None),
     "rp_sim_create": ([C.c_void_p, C.POINTER(Params), C.POINTER(C.c_void_p)], C.c_int),
+    "rp_sim_create_batch": ([C.c_void_p, C.POINTER(Params), C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)],
+                            C.c_int),
     "rp_sim_free": ([C.c_void_p], None),
     "rp_sim_run": ([C.c_void_p, C.c_void_p, STATE_CB, C.c_void_p], C.c_int),
     "rp_sim_enqueue": ([C.c_void_p, C.c_void_p], C.c_int),

@@ -134,6 +134,7 @@ struct rp_sim {
   PackedLayout L{};
   DevBuf net_size, net_first, net_rows;
   int32_t n_nets = 1;
+  std::vector<int32_t> net_bounds;  // n_nets + 1 node offsets (empty: one network)
   // shared
   DevBuf counts, beta_r, sus, classes;
   StepConsts c{};
@@ -471,10 +472,17 @@ rp_status alloc_state(rp_sim &s) {
   const int32_t n_slices = (L.q4 + 31) / 32;
   std::vector<PackedTask> tasks;
   std::vector<int32_t> first, rows, size;
-  // single network: rows [0, N)
-  first.push_back(0);
-  rows.push_back(N);
-  size.push_back(N);
+  if (s.net_bounds.empty()) {  // one network: rows [0, N)
+    first.push_back(0);
+    rows.push_back(N);
+    size.push_back(N);
+  } else {
+    for (int net = 0; net < s.n_nets; ++net) {
+      first.push_back(s.net_bounds[net]);
+      rows.push_back(s.net_bounds[net + 1] - s.net_bounds[net]);
+      size.push_back(s.net_bounds[net + 1] - s.net_bounds[net]);
+    }
+  }
   for (int net = 0; net < s.n_nets; ++net) {
     const int32_t rpt = rows_per_task(rows[net], n_slices);
     for (int32_t r0 = first[net]; r0 < first[net] + rows[net]; r0 += rpt)
@@ -719,6 +727,12 @@ RP_API void rp_params_default(rp_params *p) {
 }
 
 RP_API rp_status rp_sim_create(const rp_graph *h, const rp_params *p, rp_sim **out) {
+  return rp_sim_create_batch(h, p, nullptr, 1, out);
+}
+
+RP_API rp_status rp_sim_create_batch(const rp_graph *h, const rp_params *p,
+                                     const int32_t *net_first, int32_t n_networks,
+                                     rp_sim **out) {
   if (!h || !p || !out) {
     set_error("null argument");
     return RP_ERR_ARG;
@@ -730,6 +744,43 @@ RP_API rp_status rp_sim_create(const rp_graph *h, const rp_params *p, rp_sim **o
   }
   *out = nullptr;
   std::unique_ptr<rp_sim> s(new rp_sim());
+  if (net_first) {
+    const int32_t N = h->g.n_nodes;
+    if (n_networks < 1 || net_first[0] != 0 || net_first[n_networks] != N) {
+      set_error("network offsets must start at 0 and end at the graph's %d nodes", N);
+      return RP_ERR_ARG;
+    }
+    int32_t smallest = N;
+    for (int32_t k = 0; k < n_networks; ++k) {
+      const int32_t nk = net_first[k + 1] - net_first[k];
+      if (nk <= 0) {
+        set_error("network %d has no nodes (offsets must increase)", k);
+        return RP_ERR_ARG;
+      }
+      smallest = nk < smallest ? nk : smallest;
+    }
+    if (n_networks > 1) {
+      if (resolve_path(*p) != RP_PATH_BATCHED) {
+        set_error("a multi-network batch runs on the batched (geometric) path");
+        return RP_ERR_ARG;
+      }
+      if (p->ncls_cap) {
+        set_error("the reference's hit cap belongs to one network's index; set ncls_cap = 0 "
+                  "for a multi-network batch");
+        return RP_ERR_ARG;
+      }
+      if (p->initial_count > smallest) {
+        set_error("initial_count %d exceeds the smallest network (%d nodes)", p->initial_count,
+                  smallest);
+        return RP_ERR_ARG;
+      }
+    }
+    s->n_nets = n_networks;
+    s->net_bounds.assign(net_first, net_first + n_networks + 1);
+  } else if (n_networks != 1) {
+    set_error("network offsets missing");
+    return RP_ERR_ARG;
+  }
   RP_TRY(sim_setup(*s, h->g, *p));
   RP_TRY(alloc_state(*s));
   s->prebuilt = p->csr_mode == RP_CSR_PREBUILT;
