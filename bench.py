@@ -259,8 +259,34 @@ def run_ours(args, rank, world, local_rank):
         assert counts.shape == (T + 1, M, 4)
         # ---- CPU baseline: the C oracle on a bounded sample ----
         out["cpu_baseline"] = cpu_baseline(net, p)
+        # ---- uneven batch of independent networks, default and tuned tiles ----
+        out["uneven_batch"] = uneven_batch_leg(replay_b200, dev, timed)
         # ---- expected-value replay: forward, adjoint, beta calibration ----
         out["meanfield"] = meanfield_leg(replay_b200, g, net, p, nnz_total, hbm)
+    return out
+
+
+def uneven_batch_leg(replay_b200, dev, timed):
+    """256 independent networks (N log-uniform in [500, 50,000], 20 N
+    contacts each, 30 days, 1,440 x 30 min steps, 128 replicas each) in one
+    replay: throughput with the default tiles and after the autotuner."""
+    from replay_b200 import synthetic
+    batch = synthetic.uneven_batch()
+    p = dict(batch["params"])
+    s, e, u, v, n, off = replay_b200.batch_networks(batch["networks"])
+    t0 = time.perf_counter()
+    g = replay_b200.Graph.from_arrays(s, e, u, v, n, device=dev)
+    ingest = time.perf_counter() - t0
+    sim = replay_b200.Simulation(g, networks=off, path="batched", csr="per-step", **p)
+    nrs = n * p["M"] * p["iterations"]
+    ms0 = timed(sim, 2, 1) / 2
+    rep = sim.autotune(probe_steps=96)
+    ms1 = timed(sim, 2, 1) / 2
+    out = {"workload": batch["name"], "nodes": n, "contacts": int(len(s)), "networks": len(off) - 1,
+           "ingest_s": ingest, "ms_per_replay_default": ms0, "value_default": nrs / (ms0 / 1e3),
+           "ms_per_replay_tuned": ms1, "value_tuned": nrs / (ms1 / 1e3), "unit": UNIT, "autotune": rep}
+    sim.close()
+    g.close()
     return out
 
 

@@ -236,6 +236,16 @@ class Simulation:
         check(lib().rp_sim_run(self._h, _ptr(counts), cb, None))
         return self._shape(counts)
 
+    def autotune(self, probe_steps=48):
+        """Chooses the batched path's task height per network-size bucket by
+        timing the first probe_steps steps; returns the tuner's report."""
+        r = _lib.TuneResult()
+        check(lib().rp_sim_autotune(self._h, int(probe_steps), C.byref(r)))
+        nb = r.n_buckets
+        return {"buckets_log2": list(r.bucket_log2[:nb]), "rows_per_task": list(r.rows_per_task[:nb]),
+                "probe_steps": r.probe_steps, "probes": r.probes, "ms_default": r.ms_default,
+                "ms_tuned": r.ms_tuned}
+
     def profile(self):
         """Device time per kernel group of one eager replay (CUDA events)."""
         pr = _lib.Profile()

@@ -73,6 +73,12 @@ STATE_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_
                        C.c_int32)
 
 # Every entry point of include/replay.h with its ctypes signature.
+class TuneResult(C.Structure):
+    _fields_ = [("n_buckets", C.c_int32), ("bucket_log2", C.c_int32 * 32), ("rows_per_task", C.c_int32 * 32),
+                ("probe_steps", C.c_int32), ("probes", C.c_int32), ("ms_default", C.c_double),
+                ("ms_tuned", C.c_double)]
+
+
 SIGNATURES = {
     "rp_last_error": ([], C.c_char_p),
     "rp_version": ([], C.c_char_p),
@@ -95,6 +101,7 @@ SIGNATURES = {
     "rp_sim_create_batch": ([C.c_void_p, C.POINTER(Params), C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)],
                             C.c_int),
     "rp_sim_free": ([C.c_void_p], None),
+    "rp_sim_autotune": ([C.c_void_p, C.c_int32, C.POINTER(TuneResult)], C.c_int),
     "rp_sim_run": ([C.c_void_p, C.c_void_p, STATE_CB, C.c_void_p], C.c_int),
     "rp_sim_enqueue": ([C.c_void_p, C.c_void_p], C.c_int),
     "rp_sim_counts": ([C.c_void_p, C.c_void_p], C.c_int),

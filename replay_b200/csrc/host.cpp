@@ -6,6 +6,7 @@
 // enqueued on the device and captured once into a CUDA graph, so one replay
 // is one graph launch.  No host synchronisation inside the step loop; only
 // the (n_steps+1) x M x 4 counts leave the device.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -135,6 +136,9 @@ struct rp_sim {
   DevBuf net_size, net_first, net_rows;
   int32_t n_nets = 1;
   std::vector<int32_t> net_bounds;  // n_nets + 1 node offsets (empty: one network)
+  std::vector<int32_t> h_first, h_rows;  // per network: first row, rows
+  std::vector<int32_t> task_rows;        // per network: rows of one task
+  int32_t n_slices = 1;
   // shared
   DevBuf counts, beta_r, sus, classes;
   StepConsts c{};
@@ -357,7 +361,14 @@ rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
     set_error("the plain path supports at most 262140 replicas");
     return RP_ERR_RANGE;
   }
-  if (s.path == RP_PATH_BATCHED && s.N >= (1 << 21)) {
+  // per-(network, replica) event counters hold 21-bit fields
+  int32_t largest = s.N;
+  if (!s.net_bounds.empty()) {
+    largest = 0;
+    for (size_t k = 0; k + 1 < s.net_bounds.size(); ++k)
+      largest = std::max(largest, s.net_bounds[k + 1] - s.net_bounds[k]);
+  }
+  if (s.path == RP_PATH_BATCHED && largest >= (1 << 21)) {
     set_error("batched path counts networks of fewer than 2^21 nodes");
     return RP_ERR_RANGE;
   }
@@ -446,6 +457,27 @@ int32_t rows_per_task(int32_t n_rows, int32_t n_slices) {
   return (int32_t)rows;
 }
 
+// Tiles every network's rows into tasks of s.task_rows[net] rows x one
+// 32-column slice (a task never spans two networks: its counters flush to
+// the network's count row) and uploads them.
+rp_status upload_tasks(rp_sim &s) {
+  std::vector<PackedTask> tasks;
+  const int32_t M = s.M;
+  for (int net = 0; net < s.n_nets; ++net) {
+    const int32_t rpt = s.task_rows[net];
+    const int32_t f = s.h_first[net], e = f + s.h_rows[net];
+    for (int32_t r0 = f; r0 < e; r0 += rpt)
+      for (int32_t sl = 0; sl < s.n_slices; ++sl)
+        tasks.push_back(PackedTask{r0, std::min(r0 + rpt, e), sl, net * M});
+  }
+  if (s.tasks.bytes < sizeof(PackedTask) * tasks.size())
+    RP_TRY(s.tasks.alloc(sizeof(PackedTask) * tasks.size()));
+  RP_TRY_CUDA(cudaMemcpy(s.tasks.ptr, tasks.data(), sizeof(PackedTask) * tasks.size(),
+                         cudaMemcpyHostToDevice));
+  s.L.n_tasks = (int32_t)tasks.size();
+  return RP_OK;
+}
+
 rp_status alloc_state(rp_sim &s) {
   const int32_t N = s.N, M = s.M, T = s.T;
   const int64_t NM = (int64_t)N * M;
@@ -470,7 +502,7 @@ rp_status alloc_state(rp_sim &s) {
   while (lpr < L.q4 && lpr < 32) lpr <<= 1;
   L.lpr = lpr;
   const int32_t n_slices = (L.q4 + 31) / 32;
-  std::vector<PackedTask> tasks;
+  s.n_slices = n_slices;
   std::vector<int32_t> first, rows, size;
   if (s.net_bounds.empty()) {  // one network: rows [0, N)
     first.push_back(0);
@@ -483,14 +515,11 @@ rp_status alloc_state(rp_sim &s) {
       size.push_back(s.net_bounds[net + 1] - s.net_bounds[net]);
     }
   }
-  for (int net = 0; net < s.n_nets; ++net) {
-    const int32_t rpt = rows_per_task(rows[net], n_slices);
-    for (int32_t r0 = first[net]; r0 < first[net] + rows[net]; r0 += rpt)
-      for (int32_t sl = 0; sl < n_slices; ++sl)
-        tasks.push_back(PackedTask{r0, std::min(r0 + rpt, first[net] + rows[net]), sl,
-                                   net * M});
-  }
-  L.n_tasks = (int32_t)tasks.size();
+  s.h_first = first;
+  s.h_rows = rows;
+  // default tiles: about 3 tasks per SM over the whole batch's rows (a
+  // network smaller than a task is one task); rp_sim_autotune refines them
+  s.task_rows.assign(s.n_nets, rows_per_task(N, n_slices));
   RP_TRY(packed_prepare());
   const size_t plane = sizeof(uint32_t) * (size_t)N * L.words;
   RP_TRY(s.sa.alloc(plane));
@@ -498,9 +527,7 @@ rp_status alloc_state(rp_sim &s) {
   RP_TRY(s.mask.alloc(plane));
   RP_TRY(s.evs.alloc(plane));
   RP_TRY(s.flag.alloc(((size_t)N * L.q4 + 3) / 4 * 4));
-  RP_TRY(s.tasks.alloc(sizeof(PackedTask) * tasks.size()));
-  RP_TRY_CUDA(cudaMemcpy(s.tasks.ptr, tasks.data(), sizeof(PackedTask) * tasks.size(),
-                         cudaMemcpyHostToDevice));
+  RP_TRY(upload_tasks(s));
   const size_t per_row = (size_t)s.n_nets * M;
   RP_TRY(s.ev.alloc(sizeof(unsigned long long) * per_row * (size_t)(T > 0 ? T : 1)));
   if (s.p.p_rs > 0.0f)
@@ -961,6 +988,105 @@ RP_API rp_status rp_exposure_spmm_packed(const int32_t *d_row_ptr, const int32_t
   packed_exposure(d_row_ptr, reinterpret_cast<const int2 *>(d_entries), n_nodes, d_masks,
                   words, n_replicas, d_exposure, static_cast<cudaStream_t>(stream));
   RP_TRY_CUDA(cudaGetLastError());
+  return RP_OK;
+}
+
+// ---- tile autotuner --------------------------------------------------------
+
+RP_API rp_status rp_sim_autotune(rp_sim *s, int32_t probe_steps, rp_tune_result *out) {
+  if (!s || !out) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  if (s->path != RP_PATH_BATCHED) {
+    set_error("the autotuner tiles the batched path");
+    return RP_ERR_ARG;
+  }
+  if (s->p.record_node_states) {
+    set_error("autotune a simulation created without record_node_states");
+    return RP_ERR_ARG;
+  }
+  RP_TRY_CUDA(cudaSetDevice(s->g->device));
+  const int32_t T_full = s->T;
+  const int32_t probe = probe_steps < 1 ? 1 : (probe_steps > T_full ? T_full : probe_steps);
+  cudaEvent_t e0, e1;
+  RP_TRY_CUDA(cudaEventCreate(&e0));
+  RP_TRY_CUDA(cudaEventCreate(&e1));
+  int probes = 0;
+  // device time of the replay's first `probe` steps (second of two eager runs)
+  auto time_probe = [&](double &ms) -> rp_status {
+    s->T = probe;
+    rp_status st = RP_OK;
+    for (int rep = 0; rep < 2 && st == RP_OK; ++rep) {
+      if (rep == 1) cudaEventRecord(e0, s->stream);
+      st = s->enqueue(s->stream, nullptr, nullptr, nullptr);
+    }
+    s->T = T_full;
+    RP_TRY(st);
+    RP_TRY_CUDA(cudaEventRecord(e1, s->stream));
+    RP_TRY_CUDA(cudaEventSynchronize(e1));
+    float f = 0.0f;
+    RP_TRY_CUDA(cudaEventElapsedTime(&f, e0, e1));
+    ms = f;
+    ++probes;
+    return RP_OK;
+  };
+  // size buckets: floor(log2 rows) of each network
+  std::vector<int32_t> bucket(s->n_nets), blist;
+  for (int k = 0; k < s->n_nets; ++k) {
+    int32_t b = 0;
+    while ((2 << b) <= s->h_rows[k]) ++b;
+    bucket[k] = b;
+    if (std::find(blist.begin(), blist.end(), b) == blist.end()) blist.push_back(b);
+  }
+  std::sort(blist.begin(), blist.end(), [](int a, int b) { return a > b; });
+  if (blist.size() > 32) {
+    set_error("more than 32 network-size buckets");
+    return RP_ERR_RANGE;
+  }
+  double best = 0.0;
+  rp_status st = time_probe(best);
+  const double ms_default = best;
+  static const int32_t kCand[] = {32, 64, 128, 256, 512, 1024};
+  std::vector<int32_t> chosen(blist.size(), 0);
+  for (size_t bi = 0; bi < blist.size() && st == RP_OK; ++bi) {
+    std::vector<int32_t> keep = s->task_rows;
+    for (int32_t cand : kCand) {
+      std::vector<int32_t> saved = s->task_rows;
+      for (int k = 0; k < s->n_nets; ++k)
+        if (bucket[k] == blist[bi]) s->task_rows[k] = cand;
+      double ms = 0.0;
+      st = upload_tasks(*s);
+      if (st == RP_OK) st = time_probe(ms);
+      if (st != RP_OK) break;
+      if (ms < best * 0.98) {
+        best = ms;
+        keep = s->task_rows;
+        chosen[bi] = cand;
+      }
+      s->task_rows = saved;
+    }
+    s->task_rows = keep;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  RP_TRY(st);
+  RP_TRY(upload_tasks(*s));
+  if (s->exec) {
+    cudaGraphExecDestroy(s->exec);
+    s->exec = nullptr;
+  }
+  RP_TRY(capture(*s));
+  memset(out, 0, sizeof(*out));
+  out->n_buckets = (int32_t)blist.size();
+  for (size_t bi = 0; bi < blist.size(); ++bi) {
+    out->bucket_log2[bi] = blist[bi];
+    out->rows_per_task[bi] = chosen[bi];
+  }
+  out->probe_steps = probe;
+  out->probes = probes;
+  out->ms_default = ms_default;
+  out->ms_tuned = best;
   return RP_OK;
 }
 

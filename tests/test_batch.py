@@ -88,3 +88,23 @@ def test_batch_argument_errors():
         rb.Simulation(g, networks=off, initial_count=31, **kw)
     with pytest.raises(rb.ReplayError, match="batched"):
         rb.Simulation(g, networks=off, **dict(kw, transition="countdown"))
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_results_and_reports():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import replay_b200 as rb
+    nets = _nets(seed=90, sizes=(40, 300, 70, 1100, 520))
+    s, e, u, v, n, off = _union(nets)
+    g = rb.Graph.from_arrays(s, e, u, v, n)
+    kw = dict(M=96, iterations=30, step_size=1800.0, window=1800, start_time=nets[0]["t0"], seed=5,
+              transition="geometric", beta=7e-4, p_ei=0.3, p_ir=0.15, initial_count=3)
+    sim = rb.Simulation(g, networks=off, **kw)
+    before = sim.run()
+    rep = sim.autotune(probe_steps=10)
+    assert sorted(rep["buckets_log2"], reverse=True) == rep["buckets_log2"] == [10, 9, 8, 6, 5]
+    assert rep["probes"] == 1 + 6 * 5 and rep["ms_tuned"] <= rep["ms_default"]
+    assert all(r in (0, 32, 64, 128, 256, 512, 1024) for r in rep["rows_per_task"])
+    np.testing.assert_array_equal(sim.run(), before)
