@@ -37,9 +37,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sweep", "small", "hot"], default="sweep",
+    ap.add_argument("--workload", choices=["sweep", "small", "hot", "quiet"], default="sweep",
                     help="sweep: the replica-sweep replay (default); small: N=1,000 / 1,000 replicas; "
-                         "hot: the sweep network with 5,000 initial infected for 12 steps (profiler case)")
+                         "hot: the sweep network with 5,000 initial infected for 12 steps; quiet: its "
+                         "first 6 steps (profiler cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain-path / CPU / e2e legs")
     return ap.parse_args()
 
@@ -107,6 +108,10 @@ def workload(name):
     if name == "small":
         return synthetic.small_seir()
     net = synthetic.replica_sweep()
+    if name == "quiet":
+        # the sweep's opening steps, where almost every replica is susceptible
+        net["params"] = dict(net["params"], iterations=6)
+        net["name"] += " (first 6 steps)"
     if name == "hot":
         # every step as busy as the sweep's peak: a short replay for profiler captures
         net["params"] = dict(net["params"], initial_count=5000, iterations=12)

@@ -213,6 +213,8 @@ struct rp_sim {
       k += 2 + (p.initial_count > 0);
     } else {
       RP_TRY_CUDA(cudaMemsetAsync(ev.ptr, 0, ev.bytes, st));
+      // k_infect writes event words one by one; k_flow reads whole items
+      RP_TRY_CUDA(cudaMemsetAsync(evs.ptr, 0, evs.bytes, st));
       if (rs.ptr && p.p_rs > 0.0f) RP_TRY_CUDA(cudaMemsetAsync(rs.ptr, 0, rs.bytes, st));
       RP_TRY_CUDA(cudaMemsetAsync(init_counts.ptr, 0, init_counts.bytes, st));
       packed_init(L, sa.as<uint32_t>(), sb.as<uint32_t>(), mask.as<uint32_t>(),

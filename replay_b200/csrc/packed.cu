@@ -50,17 +50,6 @@ __device__ __forceinline__ uint32_t get4(const uint4 &v, int w) {
   return w == 0 ? v.x : (w == 1 ? v.y : (w == 2 ? v.z : v.w));
 }
 
-// 8-bit mask of the non-empty nibbles of x.
-__device__ __forceinline__ uint32_t nibble_any(uint32_t x) {
-  x |= x >> 1;
-  x |= x >> 2;
-  x &= 0x11111111u;
-  uint32_t o = 0;
-#pragma unroll
-  for (int q = 0; q < 8; ++q) o |= ((x >> (4 * q)) & 1u) << q;
-  return o;
-}
-
 __device__ __forceinline__ void or4(uint4 &a, const uint4 b) {
   a.x |= b.x;
   a.y |= b.y;
@@ -100,39 +89,112 @@ constexpr int kMaxTaskRows = 1024;  // rows of one task (host-side limit)
 constexpr int kEntCap = 1024;       // staged CSR pairs per chunk
 
 // ---------------------------------------------------------------------------
-// Per-warp scratch of k_infect (dynamic shared memory).
-struct InfectScratch {
-  int32_t off[32];        // warp scan offsets
-  uint32_t cnt4[32];      // per lane: words (phase 2) or candidate bits (phase 3)
-  int32_t rloc[32];       // task-relative row of each lane's item
-  int32_t col[32];        // column of each lane's item
-  float efmax[32];        // ef(e_max) of the item's row
-  uint32_t X[32][4];      // exposed replicas per word
-  uint32_t C[32][4];      // candidates per word (after the bound test)
-  uint32_t pl[32][4][4];  // first 4 random planes of each word
-  uint8_t have[32][4];    // planes kept (0 or 4)
-  uint32_t ev[32][4];     // infection events
+// Per-warp queue of exposed words of k_infect (dynamic shared memory):
+// entries accumulate over rows and are decided 32 at a time.
+constexpr int kInfectQueue = 160;  // 31 left over + 4 words x 32 lanes of one pass
+struct InfectQueue {
+  int32_t rloc[kInfectQueue];    // task-relative row
+  int32_t word[kInfectQueue];    // word index within the row
+  uint32_t X[kInfectQueue];      // exposed replicas of the word
+  float efmax[kInfectQueue];     // ef(e_max) of the row
+  uint32_t C[32];      // candidates after the bound test (round scratch)
+  uint32_t pl[32][4];  // first 4 random planes of each word
+  uint32_t ev[32];     // infection events of each word
+  int32_t off[32];     // warp scan offsets of the candidates
+  uint8_t have[32];    // planes kept (0 or 4)
+  int32_t n;
 };
 
-constexpr int kInfectDynSmem = kEntCap * 8 + 128 * 32 * 4 + kWarps * (int)sizeof(InfectScratch);
+constexpr int kInfectDynSmem = kEntCap * 8 + 128 * 32 * 4 + kWarps * (int)sizeof(InfectQueue);
 
-// k-th set bit over a lane's four 32-bit masks (k >= 0, exists).
-__device__ __forceinline__ void kth_bit4(const uint32_t *m, int k, int &w, int &b) {
-  w = 0;
-  while (k >= __popc(m[w])) {
-    k -= __popc(m[w]);
-    ++w;
+// Decides up to 32 queued exposed words: the bound test one word per lane
+// (phase 2), then the exact test of the surviving candidates one replica
+// per lane (phase 3); writes each word's events and flags its item.
+__device__ __forceinline__ void infect_round(InfectQueue &Q, int n, int lane, const PackedLayout &L,
+                                             const PackedTask &T, int cbase, const int32_t *s_rp,
+                                             const int2 *s_ent, const int2 *__restrict__ ent,
+                                             bool staged, int32_t e0, const float *s_beta,
+                                             const float *s_bw, const uint32_t *mask_w,
+                                             uint32_t *evs_w, uint32_t *flag32, uint32_t step,
+                                             float scale, const StepConsts &c) {
+  // ---- phase 2: bound test, one word per lane ----
+  uint32_t Cw = 0;
+  if (lane < n) {
+    const int orow = T.row_begin + Q.rloc[lane];
+    const int word = Q.word[lane];
+    // every exposed replica has P <= x <= |bs_r| ef(e_max) =: B
+    float bsmax = c.beta_r ? s_bw[word - 4 * cbase] : fabsf(c.beta);
+    if (c.sus) bsmax = __fmul_rn(bsmax, fabsf(c.sus[orow]));
+    const float B = __fmul_rn(bsmax, Q.efmax[lane]);
+    uint32_t pl[8];
+    int have = 0;
+    if (B >= 1.0f) {
+      Cw = Q.X[lane];
+    } else if (B > 0.0f) {
+      Cw = sliced_less_word(Q.X[lane], fixed64(B), c.rk, (uint32_t)orow, step, (uint32_t)word,
+                            kTagInfect, pl, have);
+    }
+    Q.have[lane] = (uint8_t)(have >= 4 ? 4 : 0);
+    if (have >= 4) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) Q.pl[lane][q] = pl[q];
+    }
   }
-  uint32_t t = m[w];
-  for (; k > 0; --k) t &= t - 1;
-  b = __ffs(t) - 1;
+  Q.C[lane] = Cw;
+  Q.ev[lane] = 0;
+  int ctotal;
+  Q.off[lane] = warp_excl_scan(__popc(Cw), lane, ctotal);
+  __syncwarp();
+  // ---- phase 3: exact test, one candidate replica per lane ----
+  for (int p = lane; p < ctotal; p += 32) {
+    const int o = find_owner(Q.off, p);
+    uint32_t t = Q.C[o];
+    for (int k = p - Q.off[o]; k > 0; --k) t &= t - 1;
+    const int b = __ffs(t) - 1;
+    const int orl = Q.rloc[o];
+    const int orow = T.row_begin + orl;
+    const int word = Q.word[o];
+    long long e = 0;
+    const int32_t ob = s_rp[orl], oe = s_rp[orl + 1];
+    for (int32_t k = ob; k < oe; ++k) {
+      const int2 q0 = staged ? s_ent[k - e0] : ent[k];
+      e += ((mask_w[(int64_t)q0.x * L.words + word] >> b) & 1u) ? q0.y : 0;
+    }
+    const float br = c.beta_r ? s_beta[(word - 4 * cbase) * 32 + b] : c.beta;
+    const float bs = c.sus ? __fmul_rn(br, c.sus[orow]) : br;
+    float ef = __ll2float_rn(e);
+    if (scale != 1.0f) ef = __fmul_rn(ef, scale);
+    const float xx = __fmul_rn(bs, ef);
+    uint32_t pl[8];
+    const int have = Q.have[o];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) pl[q] = Q.pl[o][q];
+#pragma unroll
+    for (int q = 4; q < 8; ++q) pl[q] = 0;
+    // P <= x: a uniform at or above x cannot infect (no exponential)
+    if (xx > 0.0f && xx < 1.0f &&
+        !sliced_less_one((uint32_t)b, fixed64(xx), pl, have, c.rk, (uint32_t)orow, step,
+                         (uint32_t)word, kTagInfect))
+      continue;
+    if (infect_event(one_minus_exp_neg(xx), pl, have, c.rk, (uint32_t)orow, step,
+                     (uint32_t)word, (uint32_t)b))
+      atomicOr(&Q.ev[o], 1u << b);
+  }
+  __syncwarp();
+  if (lane < n && Q.ev[lane]) {
+    const int64_t row = T.row_begin + Q.rloc[lane];
+    const int word = Q.word[lane];
+    evs_w[row * L.words + word] = Q.ev[lane];
+    const int64_t idx = row * L.q4 + (word >> 2);
+    atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
+  }
+  __syncwarp();
 }
 
-// One item (row, 4-word column) per lane; the item's global loads (the
-// neighbours' mask words and its planes) are issued together.  Exposed words
-// are then compacted across the warp for the bound test (phase 2), and the
-// surviving candidate replicas compacted again for the exact test (phase 3),
-// so that every lane works on a dense list.
+// One item (row, 4-word column) per lane gathers the OR of the neighbours'
+// mask words (its loads issued together) and queues its exposed words;
+// infect_round decides the queue 32 words at a time, so that every lane
+// works on a dense list of words and then of candidate replicas.
 __global__ void __launch_bounds__(kThreads, 3)
     k_infect(PackedLayout L, const PackedTask *__restrict__ tasks,
              const int32_t *__restrict__ row_ptr, const int2 *__restrict__ ent,
@@ -144,10 +206,13 @@ __global__ void __launch_bounds__(kThreads, 3)
   extern __shared__ __align__(16) unsigned char s_dyn[];
   int2 *s_ent = reinterpret_cast<int2 *>(s_dyn);
   float *s_beta = reinterpret_cast<float *>(s_dyn + kEntCap * sizeof(int2));
-  InfectScratch &S = reinterpret_cast<InfectScratch *>(
+  InfectQueue &Q = reinterpret_cast<InfectQueue *>(
       s_dyn + kEntCap * sizeof(int2) + 128 * 32 * sizeof(float))[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t *mask_w = reinterpret_cast<const uint32_t *>(mask_in);
+  uint32_t *evs_w = reinterpret_cast<uint32_t *>(evs);
+  if (lane == 0) Q.n = 0;
+  __syncwarp();
   for (int ti = blockIdx.x; ti < L.n_tasks; ti += gridDim.x) {
     const PackedTask T = tasks[ti];
     const int cbase = T.slice * 32;
@@ -180,7 +245,10 @@ __global__ void __launch_bounds__(kThreads, 3)
         for (int k = threadIdx.x; k < e1 - e0; k += blockDim.x) s_ent[k] = ent[e0 + k];
       __syncthreads();
       const int nitems = (r1 - r0) * ncols;
-      for (int it0 = warp * 32; it0 < nitems; it0 += kWarps * 32) {  // warp-uniform
+      // warp-uniform; one pass past the items decides what is left queued
+      // (the staged pairs change with the next chunk)
+      for (int it0 = warp * 32;; it0 += kWarps * 32) {
+        const bool flushing = it0 >= nitems;
         // ---- phase 1: gather, per lane ----
         const int it = it0 + lane;
         const bool ok = it < nitems;
@@ -223,105 +291,40 @@ __global__ void __launch_bounds__(kThreads, 3)
           efmax = __ll2float_rn(emax);
           if (scale != 1.0f) efmax = __fmul_rn(efmax, scale);
         }
-        const uint32_t wm = (X[0] ? 1u : 0u) | (X[1] ? 2u : 0u) | (X[2] ? 4u : 0u) | (X[3] ? 8u : 0u);
-        if (!__any_sync(kFull, wm != 0)) continue;
-        int total;
-        S.off[lane] = warp_excl_scan(__popc(wm), lane, total);
-        S.cnt4[lane] = wm;
-        S.rloc[lane] = rloc;
-        S.col[lane] = col;
-        S.efmax[lane] = efmax;
+        // ---- queue the exposed words ----
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
-          S.X[lane][w] = X[w];
-          S.C[lane][w] = 0;
-          S.ev[lane][w] = 0;
-        }
-        __syncwarp();
-        // ---- phase 2: bound test of the exposed words, one word per lane ----
-        for (int p = lane; p < total; p += 32) {
-          const int o = find_owner(S.off, p);
-          uint32_t m = S.cnt4[o];
-          for (int k = p - S.off[o]; k > 0; --k) m &= m - 1;
-          const int w = __ffs(m) - 1;
-          const int orow = T.row_begin + S.rloc[o];
-          const int ocol = S.col[o];
-          const int word = 4 * ocol + w;
-          const uint32_t Xw = S.X[o][w];
-          // every exposed replica has P <= x <= |bs_r| ef(e_max) =: B
-          float bsmax = c.beta_r ? s_bw[4 * (ocol - cbase) + w] : fabsf(c.beta);
-          if (c.sus) bsmax = __fmul_rn(bsmax, fabsf(c.sus[orow]));
-          const float B = __fmul_rn(bsmax, S.efmax[o]);
-          uint32_t Cw = 0;
-          uint32_t pl[8];
-          int have = 0;
-          if (B >= 1.0f) {
-            Cw = Xw;
-          } else if (B > 0.0f) {
-            Cw = sliced_less_word(Xw, fixed64(B), c.rk, (uint32_t)orow, step, (uint32_t)word,
-                                  kTagInfect, pl, have);
+          const unsigned qm = __ballot_sync(kFull, X[w] != 0u);
+          if (!qm) continue;
+          const int base = Q.n;
+          if (X[w]) {
+            const int pos = base + __popc(qm & ((1u << lane) - 1u));
+            Q.rloc[pos] = rloc;
+            Q.word[pos] = 4 * col + w;
+            Q.X[pos] = X[w];
+            Q.efmax[pos] = efmax;
           }
-          S.C[o][w] = Cw;
-          S.have[o][w] = (uint8_t)(have >= 4 ? 4 : 0);
-          if (have >= 4) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) S.pl[o][w][q] = pl[q];
-          }
+          __syncwarp();
+          if (lane == 0) Q.n = base + __popc(qm);
+          __syncwarp();
         }
-        __syncwarp();
-        // ---- phase 3: exact test of the candidates, one replica per lane ----
-        const int ncand =
-            __popc(S.C[lane][0]) + __popc(S.C[lane][1]) + __popc(S.C[lane][2]) + __popc(S.C[lane][3]);
-        int ctotal;
-        const int coff = warp_excl_scan(ncand, lane, ctotal);
-        __syncwarp();
-        S.off[lane] = coff;
-        __syncwarp();
-        for (int p = lane; p < ctotal; p += 32) {
-          const int o = find_owner(S.off, p);
-          int w, b;
-          kth_bit4(S.C[o], p - S.off[o], w, b);
-          const int orl = S.rloc[o];
-          const int orow = T.row_begin + orl;
-          const int ocol = S.col[o];
-          const int word = 4 * ocol + w;
-          long long e = 0;
-          const int32_t ob = s_rp[orl], oe = s_rp[orl + 1];
-          for (int32_t k = ob; k < oe; ++k) {
-            const int2 q0 = staged ? s_ent[k - e0] : ent[k];
-            e += ((mask_w[(int64_t)q0.x * L.words + word] >> b) & 1u) ? q0.y : 0;
+        // ---- decide full rounds (and, past the items, the remainder) ----
+        while (Q.n >= 32 || (flushing && Q.n > 0)) {
+          const int take = Q.n < 32 ? Q.n : 32;
+          infect_round(Q, take, lane, L, T, cbase, s_rp, s_ent, ent, staged, e0, s_beta, s_bw,
+                       mask_w, evs_w, flag32, step, scale, c);
+          const int rest = Q.n - take;
+          for (int i = lane; i < rest; i += 32) {
+            Q.rloc[i] = Q.rloc[take + i];
+            Q.word[i] = Q.word[take + i];
+            Q.X[i] = Q.X[take + i];
+            Q.efmax[i] = Q.efmax[take + i];
           }
-          const float br = c.beta_r ? s_beta[(4 * (ocol - cbase) + w) * 32 + b] : c.beta;
-          const float bs = c.sus ? __fmul_rn(br, c.sus[orow]) : br;
-          float ef = __ll2float_rn(e);
-          if (scale != 1.0f) ef = __fmul_rn(ef, scale);
-          const float xx = __fmul_rn(bs, ef);
-          uint32_t pl[8];
-          const int have = S.have[o][w];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) pl[q] = S.pl[o][w][q];
-#pragma unroll
-          for (int q = 4; q < 8; ++q) pl[q] = 0;
-          // P <= x: a uniform at or above x cannot infect (no exponential)
-          if (xx > 0.0f && xx < 1.0f &&
-              !sliced_less_one((uint32_t)b, fixed64(xx), pl, have, c.rk, (uint32_t)orow, step,
-                               (uint32_t)word, kTagInfect))
-            continue;
-          if (infect_event(one_minus_exp_neg(xx), pl, have, c.rk, (uint32_t)orow, step,
-                           (uint32_t)word, (uint32_t)b))
-            atomicOr(&S.ev[o][w], 1u << b);
+          __syncwarp();
+          if (lane == 0) Q.n = rest;
+          __syncwarp();
         }
-        __syncwarp();
-        if (ok) {
-          const uint32_t v0 = S.ev[lane][0], v1 = S.ev[lane][1], v2 = S.ev[lane][2],
-                         v3 = S.ev[lane][3];
-          if (v0 | v1 | v2 | v3) {
-            const int64_t idx = (int64_t)row * L.q4 + col;
-            evs[idx] = make_uint4(v0, v1, v2, v3);
-            atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
-          }
-        }
-        __syncwarp();
+        if (flushing) break;
       }
       __syncthreads();
       r0 = r1;
@@ -452,6 +455,18 @@ __global__ void __launch_bounds__(kThreads, 3)
           b4[h] = sb[idx];
         }
       }
+      // quiet items (every replica susceptible, or recovered without waning,
+      // and no infection event) need no work: skip them a warp at a time
+      bool busy = false;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const uint4 x = waning ? make_uint4(a4[h].x | b4[h].x, a4[h].y | b4[h].y, a4[h].z | b4[h].z,
+                                            a4[h].w | b4[h].w)
+                               : make_uint4(a4[h].x ^ b4[h].x, a4[h].y ^ b4[h].y, a4[h].z ^ b4[h].z,
+                                            a4[h].w ^ b4[h].w);
+        busy |= st[h] != 0 || (x.x | x.y | x.z | x.w) != 0u;
+      }
+      if (!__any_sync(kFull, busy)) continue;
 #pragma unroll
       for (int h = 0; h < 2; ++h)
         if (st[h]) {
