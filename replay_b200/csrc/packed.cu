@@ -76,6 +76,21 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int &total) {
   return incl - v;
 }
 
+// Position of the k-th (from 0) set bit of t (k < popc(t)), by halving.
+__device__ __forceinline__ int nth_set_bit(uint32_t t, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    const int c = __popc(t & ((1u << w) - 1u));
+    if (k >= c) {
+      k -= c;
+      pos += w;
+      t >>= w;
+    }
+  }
+  return pos;
+}
+
 __device__ __forceinline__ int find_owner(const int32_t *off, int p) {
   int owner = 0;
 #pragma unroll
@@ -148,9 +163,7 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, int lane, co
   // ---- phase 3: exact test, one candidate replica per lane ----
   for (int p = lane; p < ctotal; p += 32) {
     const int o = find_owner(Q.off, p);
-    uint32_t t = Q.C[o];
-    for (int k = p - Q.off[o]; k > 0; --k) t &= t - 1;
-    const int b = __ffs(t) - 1;
+    const int b = nth_set_bit(Q.C[o], p - Q.off[o]);
     const int orl = Q.rloc[o];
     const int orow = T.row_begin + orl;
     const int word = Q.word[o];
@@ -375,12 +388,14 @@ __device__ __forceinline__ void apply_word(uint32_t A, uint32_t B, uint32_t evS,
 // Per-warp queue of words with flow candidates (dynamic shared memory):
 // words are queued while the warp streams its items and drawn in full
 // 32-lane rounds, so sparse candidates do not leave lanes idle.
+constexpr int kFlowIPL = 4;      // items per lane per pass (loads in flight)
+constexpr int kFlowQueue = 160;  // 31 left over + 4 words x 32 lanes of one item group
 struct FlowQueue {
-  int32_t row[64];
-  int32_t word[64];
-  uint32_t a0[64], b0[64];  // planes at the start of the step
-  uint32_t evs[64];         // the word's infection events
-  int32_t wl[64];           // word index within the slice (counters)
+  int32_t row[kFlowQueue];
+  int32_t word[kFlowQueue];
+  uint32_t a0[kFlowQueue], b0[kFlowQueue];  // planes at the start of the step
+  uint32_t evs[kFlowQueue];                 // the word's infection events
+  int32_t wl[kFlowQueue];                   // word index within the slice (counters)
   int32_t n;
 };
 constexpr int kFlowDynSmem = 128 * 32 * 8 + kWarps * (int)sizeof(FlowQueue);
@@ -388,17 +403,18 @@ constexpr int kFlowDynSmem = 128 * 32 * 8 + kWarps * (int)sizeof(FlowQueue);
 // Draws the flows of queue entries [0, cnt) (cnt <= 32, one per lane) and
 // writes the words: infection events and flows act on disjoint state bits,
 // so both are applied here from the start-of-step planes.
-__device__ __forceinline__ void flow_round(FlowQueue &Q, int cnt, int lane, bool waning,
+__device__ __forceinline__ void flow_round(FlowQueue &Q, int base, int cnt, int lane, bool waning,
                                            const StepConsts &c, uint32_t step,
                                            unsigned long long *s_ev, uint32_t *sa_w,
                                            uint32_t *sb_w, uint32_t *mask_w, int words) {
   if (lane < cnt) {
-    const uint32_t A = Q.a0[lane], B = Q.b0[lane];
+    const int q = base + lane;
+    const uint32_t A = Q.a0[q], B = Q.b0[q];
     const uint32_t E = ~A & B, I = A & ~B, R = waning ? (A & B) : 0u;
-    const int row = Q.row[lane], word = Q.word[lane];
+    const int row = Q.row[q], word = Q.word[q];
     const uint32_t f = flow_events(E, I, R, c.th, c.rk, (uint32_t)row, step, (uint32_t)word);
     uint32_t na, nb;
-    apply_word(A, B, Q.evs[lane], f, waning, c, s_ev, Q.wl[lane], na, nb);
+    apply_word(A, B, Q.evs[q], f, waning, c, s_ev, Q.wl[q], na, nb);
     if (na != A || nb != B) {
       const int64_t wi = (int64_t)row * words + word;
       sa_w[wi] = na;
@@ -435,19 +451,20 @@ __global__ void __launch_bounds__(kThreads, 3)
     if (lane == 0) Q.n = 0;
     __syncthreads();
     const int nitems = nrows * ncols;
-    for (int it0 = warp * 64; it0 < nitems; it0 += kWarps * 64) {  // warp-uniform
-      int rl[2], cl[2];
-      bool in[2];
-      uint8_t st[2];
-      uint4 a4[2], b4[2], e4[2];
+    // warp-uniform passes of kFlowIPL items per lane, all loads issued first
+    for (int it0 = warp * 32 * kFlowIPL; it0 < nitems; it0 += kWarps * 32 * kFlowIPL) {
+      int rl[kFlowIPL], cl[kFlowIPL];
+      bool in[kFlowIPL];
+      uint8_t st[kFlowIPL];
+      uint4 a4[kFlowIPL], b4[kFlowIPL];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < kFlowIPL; ++h) {
         const int itv = it0 + 32 * h + lane;
         in[h] = itv < nitems;
         rl[h] = in[h] ? (int)dv.div((uint32_t)itv) : 0;
         cl[h] = in[h] ? itv - rl[h] * ncols : 0;
         const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
-        a4[h] = b4[h] = e4[h] = make_uint4(0, 0, 0, 0);
+        a4[h] = b4[h] = make_uint4(0, 0, 0, 0);
         st[h] = 0;
         if (in[h]) {
           st[h] = flag[idx];
@@ -459,7 +476,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       // and no infection event) need no work: skip them a warp at a time
       bool busy = false;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < kFlowIPL; ++h) {
         const uint4 x = waning ? make_uint4(a4[h].x | b4[h].x, a4[h].y | b4[h].y, a4[h].z | b4[h].z,
                                             a4[h].w | b4[h].w)
                                : make_uint4(a4[h].x ^ b4[h].x, a4[h].y ^ b4[h].y, a4[h].z ^ b4[h].z,
@@ -468,66 +485,73 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       if (!__any_sync(kFull, busy)) continue;
 #pragma unroll
-      for (int h = 0; h < 2; ++h)
+      for (int h = 0; h < kFlowIPL; ++h) {
+        const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
+        uint4 e4 = make_uint4(0, 0, 0, 0);
         if (st[h]) {
-          const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
-          e4[h] = evs[idx];
+          e4 = evs[idx];
           evs[idx] = make_uint4(0, 0, 0, 0);
           flag[idx] = 0;
         }
+        // the item's words with flow candidates go to the queue; words with
+        // infection events only are applied here
+        uint32_t cm = 0;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int h = k >> 2, w = k & 3;
-        const uint32_t A = get4(a4[h], w), B = get4(b4[h], w), ev = get4(e4[h], w);
-        const int word = 4 * (cbase + cl[h]) + w;
-        const bool valid = in[h] && word_mask(L, word) != 0u;
-        const bool cand = valid && (waning ? (A | B) : (A ^ B)) != 0u;
-        // queue the candidate words of this slot across the warp
-        const unsigned qm = __ballot_sync(kFull, cand);
-        if (qm) {
-          const int base = Q.n;
-          const int pos = base + __popc(qm & ((1u << lane) - 1u));
-          if (cand) {
-            Q.row[pos] = T.row_begin + rl[h];
-            Q.word[pos] = word;
-            Q.a0[pos] = A;
-            Q.b0[pos] = B;
-            Q.evs[pos] = ev;
-            Q.wl[pos] = 4 * cl[h] + w;
-          }
-          __syncwarp();
-          if (lane == 0) Q.n = base + __popc(qm);
-          __syncwarp();
-          if (Q.n >= 32) {
-            flow_round(Q, 32, lane, waning, c, step, s_ev, sa_w, sb_w, mask_w, L.words);
-            __syncwarp();
-            const int rest = Q.n - 32;
-            if (lane < rest) {
-              Q.row[lane] = Q.row[32 + lane];
-              Q.word[lane] = Q.word[32 + lane];
-              Q.a0[lane] = Q.a0[32 + lane];
-              Q.b0[lane] = Q.b0[32 + lane];
-              Q.evs[lane] = Q.evs[32 + lane];
-              Q.wl[lane] = Q.wl[32 + lane];
-            }
-            __syncwarp();
-            if (lane == 0) Q.n = rest;
-            __syncwarp();
+        for (int w = 0; w < 4; ++w) {
+          const uint32_t A = get4(a4[h], w), B = get4(b4[h], w), ev = get4(e4, w);
+          const int word = 4 * (cbase + cl[h]) + w;
+          const bool valid = in[h] && word_mask(L, word) != 0u;
+          const bool cand = valid && (waning ? (A | B) : (A ^ B)) != 0u;
+          if (cand) cm |= 1u << w;
+          if (valid && !cand && ev) {
+            uint32_t na, nb;
+            apply_word(A, B, ev, 0u, waning, c, s_ev, 4 * cl[h] + w, na, nb);
+            const int64_t wi = (int64_t)(T.row_begin + rl[h]) * L.words + word;
+            sa_w[wi] = na;
+            sb_w[wi] = nb;
+            mask_w[wi] = na & ~nb;
           }
         }
-        // infection events of a word without flow candidates: apply now
-        if (valid && !cand && ev) {
-          uint32_t na, nb;
-          apply_word(A, B, ev, 0u, waning, c, s_ev, 4 * cl[h] + w, na, nb);
-          const int64_t wi = (int64_t)(T.row_begin + rl[h]) * L.words + word;
-          sa_w[wi] = na;
-          sb_w[wi] = nb;
-          mask_w[wi] = na & ~nb;
+        int total;
+        const int off = warp_excl_scan(__popc(cm), lane, total);
+        if (total == 0) continue;  // warp-uniform
+        int pos = Q.n + off;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          if (!((cm >> w) & 1u)) continue;
+          Q.row[pos] = T.row_begin + rl[h];
+          Q.word[pos] = 4 * (cbase + cl[h]) + w;
+          Q.a0[pos] = get4(a4[h], w);
+          Q.b0[pos] = get4(b4[h], w);
+          Q.evs[pos] = get4(e4, w);
+          Q.wl[pos] = 4 * cl[h] + w;
+          ++pos;
         }
+        __syncwarp();
+        const int n = Q.n + total;
+        int start = 0;
+        for (; n - start >= 32; start += 32)
+          flow_round(Q, start, 32, lane, waning, c, step, s_ev, sa_w, sb_w, mask_w, L.words);
+        __syncwarp();
+        if (start > 0) {  // move the remainder (< 32 words) to the front
+          const int rest = n - start;
+          if (lane < rest) {
+            const int q = start + lane;
+            Q.row[lane] = Q.row[q];
+            Q.word[lane] = Q.word[q];
+            Q.a0[lane] = Q.a0[q];
+            Q.b0[lane] = Q.b0[q];
+            Q.evs[lane] = Q.evs[q];
+            Q.wl[lane] = Q.wl[q];
+          }
+          __syncwarp();
+        }
+        if (lane == 0) Q.n = n - start;
+        __syncwarp();
       }
     }
     __syncwarp();
-    flow_round(Q, Q.n, lane, waning, c, step, s_ev, sa_w, sb_w, mask_w, L.words);
+    flow_round(Q, 0, Q.n, lane, waning, c, step, s_ev, sa_w, sb_w, mask_w, L.words);
     __syncthreads();
     for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x) {
       const unsigned long long v = s_ev[j];

@@ -191,29 +191,30 @@ __device__ __forceinline__ uint32_t sliced_less_word(uint32_t cand, unsigned lon
   return lt;
 }
 
+// The 4 bits of replica bit b in planes x[0..3], most significant first.
+__device__ __forceinline__ uint32_t nibble_of(const uint32_t *x, uint32_t b) {
+  return (((x[0] >> b) & 1u) << 3) | (((x[1] >> b) & 1u) << 2) | (((x[2] >> b) & 1u) << 1) |
+         ((x[3] >> b) & 1u);
+}
+
 // U_b < Pf for one replica bit b of the word, first from the kept planes,
-// then from fresh ones.
+// then from fresh ones; four bits of U and of Pf are compared at a time
+// (the first differing bit decides, as in the plane-by-plane comparison).
 __device__ __forceinline__ bool sliced_less_one(uint32_t b, unsigned long long Pf,
                                                 const uint32_t pl[8], int have,
                                                 const uint32_t *rk, uint32_t node, uint32_t step,
                                                 uint32_t word, uint32_t tag) {
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    if (k >= have) break;
-    const uint32_t wb = (pl[k] >> b) & 1u;
-    const uint32_t tb = (uint32_t)(Pf >> (63 - k)) & 1u;
-    if (wb != tb) return wb < tb;
+  for (int j = 0; j < have / 4; ++j) {
+    const uint32_t u4 = nibble_of(pl + 4 * j, b);
+    const uint32_t t4 = (uint32_t)(Pf >> (60 - 4 * j)) & 0xFu;
+    if (u4 != t4) return u4 < t4;
   }
   for (int j = have / 4; j < 16; ++j) {
     uint32_t x[4];
     philox4x32_10_rk(node, step, word, tag | ((uint32_t)j << 4), rk, x);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int k = 4 * j + q;
-      const uint32_t wb = (x[q] >> b) & 1u;
-      const uint32_t tb = (uint32_t)(Pf >> (63 - k)) & 1u;
-      if (wb != tb) return wb < tb;
-    }
+    const uint32_t u4 = nibble_of(x, b);
+    const uint32_t t4 = (uint32_t)(Pf >> (60 - 4 * j)) & 0xFu;
+    if (u4 != t4) return u4 < t4;
   }
   return false;
 }
