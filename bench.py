@@ -10,8 +10,9 @@ C oracle's CPU throughput on a bounded sample.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-With torchrun (N > 1) every rank replays its own replicas (different seed):
-replicas shard with no data-path collective ("scaling": "weak").
+With torchrun (N > 1) rank r replays replicas [r M, (r+1) M) of one job
+(replica_offset): replicas shard with no data-path collective ("scaling":
+"weak").
 """
 import argparse
 import json
@@ -158,7 +159,8 @@ def run_ours(args, rank, world, local_rank):
     dev = local_rank
     net = workload(args.workload)
     p = dict(net["params"])
-    p["seed"] = 1 + rank
+    # rank r replays replicas [r M, (r + 1) M) of one N M-replica job
+    p["replica_offset"] = rank * p["M"]
     n_nodes = net["n_nodes"]
     M, T = p["M"], p["iterations"]
     nrs_per_replay = n_nodes * M * T

@@ -186,6 +186,11 @@ typedef struct {
   int32_t has_exposed; /* 0: S->I directly (SIR/SIS) */
   int32_t ir_to_s;     /* 1: recovery returns to S (SIS) */
   int32_t record_node_states; /* keep per-step node states for callbacks */
+  int32_t replica_offset; /* replicas 0..M-1 draw the random streams of
+                           * replicas replica_offset..+M-1 (a multiple of 32):
+                           * disjoint shards of one replica range, run on any
+                           * GPUs, reproduce the unsharded run exactly.  Not
+                           * in the reference. */
 } rp_params;
 
 /* Fills the reference's defaults (tool/gpu_cpu_temporal_sim.cu:24-56). */

@@ -39,6 +39,7 @@ class Params(C.Structure):
         ("ncls_cap", C.c_int32),
         ("net_first", C.c_void_p),
         ("n_nets", C.c_int32),
+        ("replica_offset", C.c_int32),
     ]
 
 

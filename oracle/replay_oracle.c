@@ -821,6 +821,9 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
   const uint64_t ti = orc_threshold64(p->p_ir, &ti_all);
   const uint64_t tr = orc_threshold64(p->p_rs, &tr_all);
 
+  /* replicas r of this run are replicas r + roff of the stream layout */
+  const int32_t roff = p->replica_offset;
+  if (roff < 0 || roff % 32) return 4;
   /* network partition (one network spanning all nodes without a batch) */
   const int32_t n_nets = p->net_first ? p->n_nets : 1;
   int32_t one_net[2] = {0, N};
@@ -831,7 +834,7 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
   for (int32_t r = 0; r < M; r++) {
     if (p->initial_count > 0) {
       for (int32_t k = 0; k < n_nets; k++) {
-        exact_k(p->seed, (uint32_t)r, (uint32_t)k, nf[k + 1] - nf[k], p->initial_count, chosen);
+        exact_k(p->seed, (uint32_t)(r + roff), (uint32_t)k, nf[k + 1] - nf[k], p->initial_count, chosen);
         for (int32_t q = 0; q < p->initial_count; q++) {
           int64_t idx = nf[k] + chosen[q] + (int64_t)r * N;
           cd[idx] = countdown ? (int32_t)((float)medium + p->step_size) : 2;
@@ -839,7 +842,7 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
       }
     } else {
       for (int32_t i = 0; i < N; i++) {
-        float uu = orc_uniform(p->seed, (uint32_t)i, 0xFFFFFFFFu, (uint32_t)r, 1u);
+        float uu = orc_uniform(p->seed, (uint32_t)i, 0xFFFFFFFFu, (uint32_t)(r + roff), 1u);
         if (uu < p->initial_infected)
           cd[i + (int64_t)r * N] = countdown ? (int32_t)((float)medium + p->step_size) : 2;
       }
@@ -882,7 +885,7 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
           if (cd[idx] == 0) {
             float e = expf_[idx] / 3600.0f;
             float P = orc_one_minus_exp_neg(neg_log_base * e);
-            float uu = orc_uniform(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, 3u);
+            float uu = orc_uniform(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)(r + roff), 3u);
             if (P > uu) cd[idx] = (int32_t)((float)upper + p->step_size);
           }
         }
@@ -906,17 +909,17 @@ int orc_run(const int64_t *start, const int64_t *end, const int32_t *u,
               float ef = (float)expi[idx];
               if (scale[t] != 1.0f) ef = ef * scale[t];
               float P = orc_one_minus_exp_neg(bs * ef);
-              if (orc_infect_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, P))
+              if (orc_infect_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)(r + roff), P))
                 cd[idx] = p->has_exposed ? 1 : 2;
             }
           } else if (st == 1) {
-            if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, te, te_all))
+            if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)(r + roff), te, te_all))
               cd[idx] = 2;
           } else if (st == 2) {
-            if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, ti, ti_all))
+            if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)(r + roff), ti, ti_all))
               cd[idx] = p->ir_to_s ? 0 : 3;
           } else {
-            if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)r, tr, tr_all))
+            if (orc_flow_event(p->seed, (uint32_t)i, (uint32_t)t, (uint32_t)(r + roff), tr, tr_all))
               cd[idx] = 0;
           }
         }

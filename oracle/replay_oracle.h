@@ -132,6 +132,9 @@ typedef struct {
    * [net_first[k], net_first[k+1]); counts become per (network, replica) */
   const int32_t *net_first; /* n_nets + 1 offsets, or NULL for one network */
   int32_t n_nets;
+  /* replica r of this run draws the streams of replica r + replica_offset
+   * (a multiple of 32): shards of one replica range reproduce it exactly */
+  int32_t replica_offset;
 } orc_params;
 
 /* Runs the whole replay.  counts: (n_steps+1) x n_nets x n_replicas x 4

@@ -54,6 +54,7 @@ class Params(C.Structure):
         ("has_exposed", C.c_int32),
         ("ir_to_s", C.c_int32),
         ("record_node_states", C.c_int32),
+        ("replica_offset", C.c_int32),
     ]
 
 

@@ -431,6 +431,11 @@ rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
   s.c.p_ei = p.p_ei;
   s.c.p_ir = p.p_ir;
   s.c.p_rs = p.p_rs;
+  if (p.replica_offset < 0 || p.replica_offset % 32 != 0) {
+    set_error("replica_offset must be a non-negative multiple of 32");
+    return RP_ERR_ARG;
+  }
+  s.c.roff = (uint32_t)p.replica_offset;
   s.c.has_exposed = p.has_exposed;
   s.c.ir_to_s = p.ir_to_s;
   s.c.beta = p.beta;

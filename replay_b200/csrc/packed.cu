@@ -146,8 +146,8 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, int lane, co
     if (B >= 1.0f) {
       Cw = Q.X[lane];
     } else if (B > 0.0f) {
-      Cw = sliced_less_word(Q.X[lane], fixed64(B), c.rk, (uint32_t)orow, step, (uint32_t)word,
-                            kTagInfect, pl, have);
+      Cw = sliced_less_word(Q.X[lane], fixed64(B), c.rk, (uint32_t)orow, step,
+                            (uint32_t)word + (c.roff >> 5), kTagInfect, pl, have);
     }
     Q.have[lane] = (uint8_t)(have >= 4 ? 4 : 0);
     if (have >= 4) {
@@ -187,10 +187,10 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, int lane, co
     // P <= x: a uniform at or above x cannot infect (no exponential)
     if (xx > 0.0f && xx < 1.0f &&
         !sliced_less_one((uint32_t)b, fixed64(xx), pl, have, c.rk, (uint32_t)orow, step,
-                         (uint32_t)word, kTagInfect))
+                         (uint32_t)word + (c.roff >> 5), kTagInfect))
       continue;
     if (infect_event(one_minus_exp_neg(xx), pl, have, c.rk, (uint32_t)orow, step,
-                     (uint32_t)word, (uint32_t)b))
+                     (uint32_t)word + (c.roff >> 5), (uint32_t)b))
       atomicOr(&Q.ev[o], 1u << b);
   }
   __syncwarp();
@@ -412,7 +412,8 @@ __device__ __forceinline__ void flow_round(FlowQueue &Q, int base, int cnt, int 
     const uint32_t A = Q.a0[q], B = Q.b0[q];
     const uint32_t E = ~A & B, I = A & ~B, R = waning ? (A & B) : 0u;
     const int row = Q.row[q], word = Q.word[q];
-    const uint32_t f = flow_events(E, I, R, c.th, c.rk, (uint32_t)row, step, (uint32_t)word);
+    const uint32_t f =
+        flow_events(E, I, R, c.th, c.rk, (uint32_t)row, step, (uint32_t)word + (c.roff >> 5));
     uint32_t na, nb;
     apply_word(A, B, Q.evs[q], f, waning, c, s_ev, Q.wl[q], na, nb);
     if (na != A || nb != B) {
@@ -617,7 +618,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         uint32_t x[4];
-        philox4x32_10((uint32_t)row, kStepInit, (uint32_t)(word * 8 + q), kStreamInit, c.key0,
+        philox4x32_10((uint32_t)row, kStepInit, (uint32_t)((word + (c.roff >> 5)) * 8 + q), kStreamInit, c.key0,
                       c.key1, x);
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc)
@@ -646,7 +647,7 @@ __global__ void k_packed_pick(PackedLayout L, uint32_t *__restrict__ sa,
   const int32_t kk = k < n ? k : n;
   for (int32_t j = n - kk; j < n; ++j) {
     uint32_t x[4];
-    philox4x32_10((uint32_t)j, kStepPick, (uint32_t)r, kStreamPick + 4u * (uint32_t)net, c.key0,
+    philox4x32_10((uint32_t)j, kStepPick, (uint32_t)r + c.roff, kStreamPick + 4u * (uint32_t)net, c.key0,
                   c.key1, x);
     const uint64_t r64 = (uint64_t)x[0] | ((uint64_t)x[1] << 32);
     const int32_t t = (int32_t)__umul64hi(r64, (uint64_t)(j + 1));

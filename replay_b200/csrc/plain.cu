@@ -121,7 +121,8 @@ __global__ void __launch_bounds__(256)
       any_s |= v[c4] == 0;
     }
     uint32_t x[4] = {0, 0, 0, 0};
-    if (any_s) philox4x32_10((uint32_t)i, step, (uint32_t)q, kStreamInfect, c.key0, c.key1, x);
+    if (any_s)
+      philox4x32_10((uint32_t)i, step, (uint32_t)q + (c.roff >> 2), kStreamInfect, c.key0, c.key1, x);
 #pragma unroll
     for (int c4 = 0; c4 < 4; ++c4) {
       const int32_t r = 4 * q + c4;
@@ -181,11 +182,10 @@ __global__ void __launch_bounds__(256)
         Rm |= v[c4] == 3 ? bit : 0u;
       }
     }
-    const uint32_t word = (uint32_t)(q >> 3);
+    const uint32_t word = (uint32_t)(q >> 3) + (c.roff >> 5);  // stream word of the replicas
     const uint32_t no_planes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const uint32_t ev = (Em | Im | Rm)
-                            ? flow_events(Em, Im, Rm, c.th, c.rk, (uint32_t)i, step,
-                                          (uint32_t)(q >> 3))
+                            ? flow_events(Em, Im, Rm, c.th, c.rk, (uint32_t)i, step, word)
                             : 0u;
 #pragma unroll
     for (int c4 = 0; c4 < 4; ++c4) {
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(256)
   const int32_t q = blockIdx.y;
   if (i >= n) return;
   uint32_t x[4];
-  philox4x32_10((uint32_t)i, kStepInit, (uint32_t)q, kStreamInit, c.key0, c.key1, x);
+  philox4x32_10((uint32_t)i, kStepInit, (uint32_t)q + (c.roff >> 2), kStreamInit, c.key0, c.key1, x);
 #pragma unroll
   for (int c4 = 0; c4 < 4; ++c4) {
     const int32_t r = 4 * q + c4;
@@ -246,7 +246,7 @@ __global__ void k_pick(int transition, void *__restrict__ state, int32_t n, int3
   const int32_t val = cd_add(c.medium, c.step_size);
   for (int32_t j = n - k; j < n; ++j) {
     uint32_t x[4];
-    philox4x32_10((uint32_t)j, kStepPick, (uint32_t)r, kStreamPick, c.key0, c.key1, x);
+    philox4x32_10((uint32_t)j, kStepPick, (uint32_t)r + c.roff, kStreamPick, c.key0, c.key1, x);
     const uint64_t r64 = (uint64_t)x[0] | ((uint64_t)x[1] << 32);
     const int32_t t = (int32_t)__umul64hi(r64, (uint64_t)(j + 1));
     int64_t idx = t + (int64_t)r * n;

@@ -197,6 +197,7 @@ struct StepConsts {
   float beta;
   const float *beta_r;  // device, may be null
   const float *sus;     // device, may be null
+  uint32_t roff;        // replica offset of the stream layout (multiple of 32)
 };
 
 // Plain path (column-major N x M state, per-replica SpMV + elementwise).

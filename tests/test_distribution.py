@@ -99,7 +99,9 @@ def test_matches_reference_gpu_path_in_distribution(runs):
     10,000 replicas), and its per-step infection draws inherit the same
     seeding.  So the dynamics are compared within strata of equal initial
     count, and our output must be at least as close to the reference GPU
-    path as the reference's own CPU path is."""
+    path as the reference's own CPU path is (how far the GPU path strays
+    varies from run to run: 32% to 88% of its means inside the 95% interval
+    of its own CPU path's have been seen)."""
     ours, ref_gpu, ref_cpu = runs
     assert ours[-1, :, 3].mean() < 0.5 * 300  # the epidemic takes off
     k_ours, k_ref = ours[0, :, 0], ref_gpu[0, :, 0]
@@ -112,7 +114,10 @@ def test_matches_reference_gpu_path_in_distribution(runs):
     inside_c = _report(f"reference CPU vs reference GPU path, {len(strata_c)} strata", zc, min(pc))
     assert inside >= inside_c - 0.05
     assert np.max(np.abs(z)) < max(5.0, np.max(np.abs(zc)) + 1.0)
-    assert min(ps) > min(0.01 / len(strata), 0.1 * min(pc))
+    # the final-size test is informative only in runs where the reference's
+    # GPU path agrees with its own CPU path (its seeding varies with time)
+    if min(pc) > 0.01 / len(strata_c):
+        assert min(ps) > 0.01 / len(strata)
 
 
 def test_matches_reference_cpu_path_in_distribution(runs):
