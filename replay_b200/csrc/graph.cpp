@@ -2,8 +2,8 @@
 //
 // Replaces tool/temporal_contact_matrix.c (parse_edgelist_build_intervals
 // :148-321, count_valid_edges :122-143, parse_iso8601_to_unix :95-120,
-// get_or_create_node_index :328-356) and the NCLS build
-// (tool/ncls/ncls/src/intervaldb.c:227-326).
+// get_or_create_node_index :328-356); the index itself is built on the
+// device (ingest.cu).
 //
 // The file format and its acceptance rules are the reference's:
 //  * line 1 starts with "NODE_LIST" + blank; its tokens are non-negative
@@ -252,43 +252,6 @@ struct IdMap {
   }
 };
 
-// Stable LSD radix sort of (key, value) by key, 16-bit digits.
-void radix_sort_u64(std::vector<uint64_t> &key, std::vector<uint32_t> &val) {
-  const size_t n = key.size();
-  std::vector<uint64_t> k2(n);
-  std::vector<uint32_t> v2(n);
-  std::vector<size_t> cnt(65536);
-  for (int sh = 0; sh < 64; sh += 16) {
-    std::fill(cnt.begin(), cnt.end(), 0);
-    for (size_t i = 0; i < n; ++i) cnt[(key[i] >> sh) & 0xFFFF]++;
-    bool trivial = false;
-    for (size_t b = 0; b < 65536; ++b)
-      if (cnt[b] == n) trivial = true;
-    if (trivial) continue;
-    size_t acc = 0;
-    for (size_t b = 0; b < 65536; ++b) {
-      size_t c = cnt[b];
-      cnt[b] = acc;
-      acc += c;
-    }
-    for (size_t i = 0; i < n; ++i) {
-      size_t pos = cnt[(key[i] >> sh) & 0xFFFF]++;
-      k2[pos] = key[i];
-      v2[pos] = val[i];
-    }
-    key.swap(k2);
-    val.swap(v2);
-  }
-}
-
-int bit_width_u64(uint64_t x) {
-  int b = 0;
-  while (x) {
-    ++b;
-    x >>= 1;
-  }
-  return b;
-}
 
 }  // namespace
 
@@ -460,133 +423,6 @@ rp_status parse_contact_file(const char *path, int32_t &n_nodes,
         }
       });
     for (auto &th : pool) th.join();
-  }
-  return RP_OK;
-}
-
-// ---------------------------------------------------------------------------
-rp_status graph_build(Graph &g, std::vector<int64_t> &start,
-                      std::vector<int64_t> &end, std::vector<int32_t> &u,
-                      std::vector<int32_t> &v, int32_t n_nodes) {
-  const int64_t n = (int64_t)start.size();
-  g.n_nodes = n_nodes;
-  g.n_contacts = n;
-  if (n > (int64_t)INT32_MAX) {
-    set_error("too many contacts");
-    return RP_ERR_RANGE;
-  }
-  // Stored coordinates: the reference database keeps intervals with a
-  // negative start mirrored as (-end, -(int)start) (ALL_POSITIVE_ORIENTATION,
-  // intervaldb.c:233-235 and :412-424).
-  for (int64_t i = 0; i < n; ++i) {
-    if (start[i] < 0) {
-      const int64_t s = start[i];
-      start[i] = -end[i];
-      end[i] = -(int64_t)(int32_t)s;
-    }
-  }
-  // Order by (start asc, end desc), ties in file order: the reference's
-  // qsort (imstart_qsort_cmp, intervaldb.c:30-46) is glibc's stable merge sort.
-  std::vector<uint32_t> perm(n);
-  for (int64_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
-  if (n > 0) {
-    int64_t smin = start[0], smax = start[0], emin = end[0], emax = end[0];
-    for (int64_t i = 1; i < n; ++i) {
-      smin = std::min(smin, start[i]);
-      smax = std::max(smax, start[i]);
-      emin = std::min(emin, end[i]);
-      emax = std::max(emax, end[i]);
-    }
-    const uint64_t srange = (uint64_t)smax - (uint64_t)smin;
-    const uint64_t erange = (uint64_t)emax - (uint64_t)emin;
-    const int sb = bit_width_u64(srange), eb = bit_width_u64(erange);
-    std::vector<uint64_t> key(n);
-    if (sb + eb <= 64) {
-      for (int64_t i = 0; i < n; ++i)
-        key[i] = (eb == 64 ? 0 : (((uint64_t)start[i] - (uint64_t)smin) << eb)) |
-                 ((uint64_t)emax - (uint64_t)end[i]);
-      radix_sort_u64(key, perm);
-    } else {
-      for (int64_t i = 0; i < n; ++i) key[i] = (uint64_t)emax - (uint64_t)end[i];
-      radix_sort_u64(key, perm);
-      for (int64_t i = 0; i < n; ++i) key[i] = (uint64_t)start[perm[i]] - (uint64_t)smin;
-      radix_sort_u64(key, perm);
-    }
-    g.t_min = smin;
-    g.t_max = emax;
-  }
-  std::vector<int64_t> ss(n), se(n);
-  std::vector<int32_t> su(n), sv(n);
-  for (int64_t i = 0; i < n; ++i) {
-    ss[i] = start[perm[i]];
-    se[i] = end[perm[i]];
-    su[i] = u[perm[i]];
-    sv[i] = v[perm[i]];
-  }
-  // nlists of the nested containment list (intervaldb.c:243-320): one header
-  // per interval with a child plus one per restart of the parent chain, i.e.
-  // (top-level intervals - 1) + (intervals with a child).  i nests in the
-  // nearest open ancestor containing it; identical intervals do not nest.
-  {
-    std::vector<int64_t> chain;
-    chain.reserve(64);
-    std::vector<uint8_t> has_child(n, 0);
-    int64_t n_top = 0;
-    for (int64_t i = 0; i < n; ++i) {
-      while (!chain.empty()) {
-        const int64_t p = chain.back();
-        const bool outside = se[i] > se[p] || (se[i] == se[p] && ss[i] == ss[p]);
-        if (!outside) break;
-        chain.pop_back();
-      }
-      if (chain.empty())
-        ++n_top;
-      else
-        has_child[chain.back()] = 1;
-      chain.push_back(i);
-    }
-    int64_t parents = 0;
-    for (int64_t i = 0; i < n; ++i) parents += has_child[i];
-    g.nlists = n > 0 ? (n_top - 1) + parents : 0;
-  }
-  // Duration classes, stable: class 0 durations <= 1, class c in (2^(c-1), 2^c].
-  std::vector<uint8_t> cls(n);
-  std::vector<int64_t> cnt(kClasses + 1, 0);
-  for (int64_t i = 0; i < n; ++i) {
-    const int64_t d = se[i] - ss[i];
-    int c = 0;
-    if (d > 1) c = bit_width_u64((uint64_t)(d - 1));
-    cls[i] = (uint8_t)c;
-    cnt[c + 1]++;
-  }
-  g.class_off.assign(kClasses + 1, 0);
-  for (int c = 0; c < kClasses; ++c) g.class_off[c + 1] = g.class_off[c] + cnt[c + 1];
-  g.n_classes_used = 0;
-  for (int c = 0; c < kClasses; ++c) g.n_classes_used += cnt[c + 1] > 0;
-  std::vector<int64_t> pos(g.class_off.begin(), g.class_off.end() - 1);
-  std::vector<int64_t> cs(n), ce(n);
-  std::vector<int32_t> cu(n), cv(n), cr(n);
-  for (int64_t i = 0; i < n; ++i) {
-    const int64_t p = pos[cls[i]]++;
-    cs[p] = ss[i];
-    ce[p] = se[i];
-    cu[p] = su[i];
-    cv[p] = sv[i];
-    cr[p] = (int32_t)i;
-  }
-  g.h_cs = cs;
-  RP_TRY_CUDA(cudaSetDevice(g.device));
-  RP_TRY(g.cs.alloc(sizeof(int64_t) * n));
-  RP_TRY(g.ce.alloc(sizeof(int64_t) * n));
-  RP_TRY(g.cu.alloc(sizeof(int32_t) * n));
-  RP_TRY(g.cv.alloc(sizeof(int32_t) * n));
-  RP_TRY(g.crank.alloc(sizeof(int32_t) * n));
-  if (n > 0) {
-    RP_TRY_CUDA(cudaMemcpy(g.cs.ptr, cs.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
-    RP_TRY_CUDA(cudaMemcpy(g.ce.ptr, ce.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
-    RP_TRY_CUDA(cudaMemcpy(g.cu.ptr, cu.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
-    RP_TRY_CUDA(cudaMemcpy(g.cv.ptr, cv.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
-    RP_TRY_CUDA(cudaMemcpy(g.crank.ptr, cr.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
   }
   return RP_OK;
 }

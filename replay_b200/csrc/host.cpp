@@ -593,7 +593,8 @@ RP_API rp_status rp_graph_load_text(const char *path, int device, rp_graph **out
   h->g.device = device;
   h->g.n_index = n_index;
   h->g.n_malformed = malformed;
-  RP_TRY(graph_build(h->g, st, en, u, v, n_nodes));
+  RP_TRY(graph_build_device(h->g, st.data(), en.data(), u.data(), v.data(), (int64_t)st.size(),
+                            n_nodes));
   *out = h.release();
   return RP_OK;
 }
@@ -647,7 +648,6 @@ RP_API rp_status rp_graph_from_arrays(const int64_t *start, const int64_t *end,
     return RP_ERR_ARG;
   }
   *out = nullptr;
-  std::vector<int64_t> st(start, start + n_contacts), en(end, end + n_contacts);
   std::vector<int32_t> uu(n_contacts), vv(n_contacts);
   std::vector<uint8_t> seen(n_nodes, 0);
   int32_t n_index = 0;
@@ -666,7 +666,7 @@ RP_API rp_status rp_graph_from_arrays(const int64_t *start, const int64_t *end,
   std::unique_ptr<rp_graph> h(new rp_graph());
   h->g.device = device;
   h->g.n_index = n_index;
-  RP_TRY(graph_build(h->g, st, en, uu, vv, n_nodes));
+  RP_TRY(graph_build_device(h->g, start, end, uu.data(), vv.data(), n_contacts, n_nodes));
   *out = h.release();
   return RP_OK;
 }

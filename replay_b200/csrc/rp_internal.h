@@ -113,9 +113,10 @@ rp_status parse_contact_file(const char *path, int32_t &n_nodes,
                              std::vector<int64_t> &start,
                              std::vector<int64_t> &end, std::vector<int32_t> &u,
                              std::vector<int32_t> &v);
-rp_status graph_build(Graph &g, std::vector<int64_t> &start,
-                      std::vector<int64_t> &end, std::vector<int32_t> &u,
-                      std::vector<int32_t> &v, int32_t n_nodes);
+// Builds the device interval index of n contacts given in host memory
+// (u[k] <= v[k]); ingest.cu.
+rp_status graph_build_device(Graph &g, const int64_t *start, const int64_t *end,
+                             const int32_t *u, const int32_t *v, int64_t n, int32_t n_nodes);
 
 // Plans the query of one window: candidate ranges appended to `ranges`.
 void plan_window(const Graph &g, int64_t ws, int64_t we, float scale,

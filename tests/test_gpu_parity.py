@@ -171,3 +171,28 @@ def test_node_states_callback(rb, oracle):
                                 node_states=True, **_oracle_kw(kw))
     np.testing.assert_array_equal(counts, want_c)
     np.testing.assert_array_equal(np.stack(seen), want_s)
+
+
+@pytest.mark.parametrize("negative", [False, True])
+def test_device_index_matches_oracle_across_sort_tiles(rb, oracle, negative):
+    """300k contacts (73 radix tiles, 74 nesting chunks) with many exact
+    ties and nested intervals: nlists and window CSRs match the oracle."""
+    rng = np.random.default_rng(7 + negative)
+    n, nodes = 300_000, 5000
+    base = -3 * 86400 if negative else 946684800
+    start = base + rng.integers(0, 86400, n) // 60 * 60  # minute grid: many equal starts
+    end = start + rng.choice([1, 60, 600, 3600, 7200, 40000], n)  # few durations: ties and nesting
+    u = rng.integers(0, nodes, n).astype(np.int32)
+    v = ((u + 1 + rng.integers(0, nodes - 1, n)) % nodes).astype(np.int32)
+    g = rb.Graph.from_arrays(start, end, u, v, nodes)
+    ss, se, su, sv, perm, nl = oracle.sorted_index(start, end, np.minimum(u, v), np.maximum(u, v))
+    assert g.info["nlists"] == nl
+    for ws in (base, base + 3 * 3600 + 17, base + 20 * 3600):
+        for cap in (True, False):
+            rp, col, val, nh = rb.window_csr(g, ws, ws + 3600, 1.0, "f32", cap)
+            hits = oracle.window_hits(ss, se, nl if cap else len(ss), ws, ws + 3600)
+            orp, ocol, oval = oracle.csr_f32(ss, se, su, sv, hits, nodes, ws, ws + 3600, np.float32(1.0))
+            assert nh == len(hits)
+            np.testing.assert_array_equal(rp, orp)
+            np.testing.assert_array_equal(col, ocol)
+            np.testing.assert_array_equal(val.view(np.int32), oval.view(np.int32))
