@@ -270,13 +270,19 @@ __global__ void __launch_bounds__(256)
 __global__ void k_class_keys(const int64_t *__restrict__ ss, const int64_t *__restrict__ se,
                              int64_t n, unsigned long long *__restrict__ key,
                              unsigned long long *__restrict__ class_cnt) {
+  __shared__ unsigned int h[kClasses];
+  for (int c = threadIdx.x; c < kClasses; c += blockDim.x) h[c] = 0;
+  __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t d = se[i] - ss[i];
     const int c = d > 1 ? 64 - __clzll((long long)(d - 1)) : 0;
     key[i] = (unsigned long long)c;
-    atomicAdd(&class_cnt[c], 1ull);
+    atomicAdd(&h[c], 1u);
   }
+  __syncthreads();
+  for (int c = threadIdx.x; c < kClasses; c += blockDim.x)
+    if (h[c]) atomicAdd(&class_cnt[c], (unsigned long long)h[c]);
 }
 
 int grid_of(int64_t n, int threads) {

@@ -389,13 +389,10 @@ __device__ __forceinline__ void apply_word(uint32_t A, uint32_t B, uint32_t evS,
 // words are queued while the warp streams its items and drawn in full
 // 32-lane rounds, so sparse candidates do not leave lanes idle.
 constexpr int kFlowIPL = 4;      // items per lane per pass (loads in flight)
-constexpr int kFlowQueue = 160;  // 31 left over + 4 words x 32 lanes of one item group
+constexpr int kFlowQueue = 576;  // 31 left over + 4 words x kFlowIPL items x 32 lanes (+ pad)
 struct FlowQueue {
   int32_t row[kFlowQueue];
-  int32_t word[kFlowQueue];
-  uint32_t a0[kFlowQueue], b0[kFlowQueue];  // planes at the start of the step
-  uint32_t evs[kFlowQueue];                 // the word's infection events
-  int32_t wl[kFlowQueue];                   // word index within the slice (counters)
+  uint16_t word[kFlowQueue];  // word index within the row
   int32_t n;
 };
 constexpr int kFlowDynSmem = 128 * 32 * 8 + kWarps * (int)sizeof(FlowQueue);
@@ -403,21 +400,23 @@ constexpr int kFlowDynSmem = 128 * 32 * 8 + kWarps * (int)sizeof(FlowQueue);
 // Draws the flows of queue entries [0, cnt) (cnt <= 32, one per lane) and
 // writes the words: infection events and flows act on disjoint state bits,
 // so both are applied here from the start-of-step planes.
-__device__ __forceinline__ void flow_round(FlowQueue &Q, int base, int cnt, int lane, bool waning,
-                                           const StepConsts &c, uint32_t step,
+__device__ __forceinline__ void flow_round(const FlowQueue &Q, int base, int cnt, int lane,
+                                           bool waning, const StepConsts &c, uint32_t step,
                                            unsigned long long *s_ev, uint32_t *sa_w,
-                                           uint32_t *sb_w, uint32_t *mask_w, int words) {
+                                           uint32_t *sb_w, uint32_t *mask_w, uint32_t *evs_w,
+                                           int words, int cbase) {
   if (lane < cnt) {
     const int q = base + lane;
-    const uint32_t A = Q.a0[q], B = Q.b0[q];
-    const uint32_t E = ~A & B, I = A & ~B, R = waning ? (A & B) : 0u;
     const int row = Q.row[q], word = Q.word[q];
+    const int64_t wi = (int64_t)row * words + word;
+    const uint32_t A = sa_w[wi], B = sb_w[wi], ev = evs_w[wi];
+    if (ev) evs_w[wi] = 0u;
+    const uint32_t E = ~A & B, I = A & ~B, R = waning ? (A & B) : 0u;
     const uint32_t f =
         flow_events(E, I, R, c.th, c.rk, (uint32_t)row, step, (uint32_t)word + (c.roff >> 5));
     uint32_t na, nb;
-    apply_word(A, B, Q.evs[q], f, waning, c, s_ev, Q.wl[q], na, nb);
+    apply_word(A, B, ev, f, waning, c, s_ev, word - 4 * cbase, na, nb);
     if (na != A || nb != B) {
-      const int64_t wi = (int64_t)row * words + word;
       sa_w[wi] = na;
       sb_w[wi] = nb;
       mask_w[wi] = na & ~nb;
@@ -452,8 +451,13 @@ __global__ void __launch_bounds__(kThreads, 3)
     if (lane == 0) Q.n = 0;
     __syncthreads();
     const int nitems = nrows * ncols;
-    // warp-uniform passes of kFlowIPL items per lane, all loads issued first
-    for (int it0 = warp * 32 * kFlowIPL; it0 < nitems; it0 += kWarps * 32 * kFlowIPL) {
+    uint32_t *evs_w = reinterpret_cast<uint32_t *>(evs);
+    // warp-uniform passes of kFlowIPL items per lane, all loads issued
+    // first; candidate words are queued, and full rounds of 32 decided after
+    // the pass (one pass past the items decides the rest; one call site of
+    // flow_round keeps the kernel small)
+    for (int it0 = warp * 32 * kFlowIPL;; it0 += kWarps * 32 * kFlowIPL) {
+      const bool flushing = it0 >= nitems;
       int rl[kFlowIPL], cl[kFlowIPL];
       bool in[kFlowIPL];
       uint8_t st[kFlowIPL];
@@ -476,83 +480,86 @@ __global__ void __launch_bounds__(kThreads, 3)
       // quiet items (every replica susceptible, or recovered without waning,
       // and no infection event) need no work: skip them a warp at a time
       bool busy = false;
+      uint32_t cm[kFlowIPL];
+      int cnt = 0;
 #pragma unroll
       for (int h = 0; h < kFlowIPL; ++h) {
-        const uint4 x = waning ? make_uint4(a4[h].x | b4[h].x, a4[h].y | b4[h].y, a4[h].z | b4[h].z,
-                                            a4[h].w | b4[h].w)
-                               : make_uint4(a4[h].x ^ b4[h].x, a4[h].y ^ b4[h].y, a4[h].z ^ b4[h].z,
-                                            a4[h].w ^ b4[h].w);
-        busy |= st[h] != 0 || (x.x | x.y | x.z | x.w) != 0u;
+        cm[h] = 0;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const uint32_t A = get4(a4[h], w), B = get4(b4[h], w);
+          const bool valid = in[h] && word_mask(L, 4 * (cbase + cl[h]) + w) != 0u;
+          if (valid && (waning ? (A | B) : (A ^ B)) != 0u) cm[h] |= 1u << w;
+        }
+        cnt += __popc(cm[h]);
+        busy |= st[h] != 0 || cm[h] != 0;
       }
-      if (!__any_sync(kFull, busy)) continue;
+      if (!flushing && !__any_sync(kFull, busy)) continue;
+      // infection events: words without flow candidates are applied here;
+      // the queued words' events are read (and cleared) by their round
 #pragma unroll
       for (int h = 0; h < kFlowIPL; ++h) {
+        if (!st[h]) continue;
         const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
-        uint4 e4 = make_uint4(0, 0, 0, 0);
-        if (st[h]) {
-          e4 = evs[idx];
-          evs[idx] = make_uint4(0, 0, 0, 0);
-          flag[idx] = 0;
-        }
-        // the item's words with flow candidates go to the queue; words with
-        // infection events only are applied here
-        uint32_t cm = 0;
+        const uint4 e4 = evs[idx];
+        flag[idx] = 0;
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
-          const uint32_t A = get4(a4[h], w), B = get4(b4[h], w), ev = get4(e4, w);
+          const uint32_t ev = get4(e4, w);
+          if (!ev || ((cm[h] >> w) & 1u)) continue;
           const int word = 4 * (cbase + cl[h]) + w;
-          const bool valid = in[h] && word_mask(L, word) != 0u;
-          const bool cand = valid && (waning ? (A | B) : (A ^ B)) != 0u;
-          if (cand) cm |= 1u << w;
-          if (valid && !cand && ev) {
-            uint32_t na, nb;
-            apply_word(A, B, ev, 0u, waning, c, s_ev, 4 * cl[h] + w, na, nb);
-            const int64_t wi = (int64_t)(T.row_begin + rl[h]) * L.words + word;
-            sa_w[wi] = na;
-            sb_w[wi] = nb;
-            mask_w[wi] = na & ~nb;
-          }
+          const int64_t wi = (int64_t)(T.row_begin + rl[h]) * L.words + word;
+          uint32_t na, nb;
+          apply_word(get4(a4[h], w), get4(b4[h], w), ev, 0u, waning, c, s_ev, 4 * cl[h] + w, na,
+                     nb);
+          sa_w[wi] = na;
+          sb_w[wi] = nb;
+          mask_w[wi] = na & ~nb;
+          evs_w[wi] = 0u;
         }
-        int total;
-        const int off = warp_excl_scan(__popc(cm), lane, total);
-        if (total == 0) continue;  // warp-uniform
-        int pos = Q.n + off;
+      }
+      // queue the candidate words of the pass (one scan)
+      int total;
+      int pos = warp_excl_scan(cnt, lane, total);
+      if (total > 0) {  // warp-uniform
+        pos += Q.n;
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
-          if (!((cm >> w) & 1u)) continue;
-          Q.row[pos] = T.row_begin + rl[h];
-          Q.word[pos] = 4 * (cbase + cl[h]) + w;
-          Q.a0[pos] = get4(a4[h], w);
-          Q.b0[pos] = get4(b4[h], w);
-          Q.evs[pos] = get4(e4, w);
-          Q.wl[pos] = 4 * cl[h] + w;
-          ++pos;
-        }
-        __syncwarp();
-        const int n = Q.n + total;
-        int start = 0;
-        for (; n - start >= 32; start += 32)
-          flow_round(Q, start, 32, lane, waning, c, step, s_ev, sa_w, sb_w, mask_w, L.words);
-        __syncwarp();
-        if (start > 0) {  // move the remainder (< 32 words) to the front
-          const int rest = n - start;
-          if (lane < rest) {
-            const int q = start + lane;
-            Q.row[lane] = Q.row[q];
-            Q.word[lane] = Q.word[q];
-            Q.a0[lane] = Q.a0[q];
-            Q.b0[lane] = Q.b0[q];
-            Q.evs[lane] = Q.evs[q];
-            Q.wl[lane] = Q.wl[q];
-          }
-          __syncwarp();
-        }
-        if (lane == 0) Q.n = n - start;
+        for (int h = 0; h < kFlowIPL; ++h)
+#pragma unroll
+          for (int w = 0; w < 4; ++w)
+            if ((cm[h] >> w) & 1u) {
+              Q.row[pos] = T.row_begin + rl[h];
+              Q.word[pos] = (uint16_t)(4 * (cbase + cl[h]) + w);
+              ++pos;
+            }
         __syncwarp();
       }
+      const int n = Q.n + total;
+      int start = 0;
+      for (; n - start >= 32 || (flushing && n - start > 0); start += 32)
+        flow_round(Q, start, min(32, n - start), lane, waning, c, step, s_ev, sa_w, sb_w, mask_w,
+                   evs_w, L.words, cbase);
+      __syncwarp();
+      const int rest = max(n - start, 0);
+      if (start > 0 && rest > 0) {  // move the remainder (< 32 words) to the front
+        const int q = start + lane;
+        int32_t r0 = 0;
+        uint16_t w0 = 0;
+        if (lane < rest) {
+          r0 = Q.row[q];
+          w0 = Q.word[q];
+        }
+        __syncwarp();
+        if (lane < rest) {
+          Q.row[lane] = r0;
+          Q.word[lane] = w0;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) Q.n = rest;
+      __syncwarp();
+      if (flushing) break;
     }
-    __syncwarp();
-    flow_round(Q, 0, Q.n, lane, waning, c, step, s_ev, sa_w, sb_w, mask_w, L.words);
     __syncthreads();
     for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x) {
       const unsigned long long v = s_ev[j];
