@@ -230,6 +230,19 @@ typedef int (*rp_state_cb)(void *user, int32_t step_index, int64_t timestamp,
 RP_API rp_status rp_sim_run(rp_sim *s, int32_t *counts, rp_state_cb cb,
                             void *user);
 
+/* Node-state CSV text, formatted on the device: `cb` receives, for every
+ * recorded step (step_index 0 the initial state), the lines
+ * "time,simulation_id,node_id,state\n" (state susceptible, incubating,
+ * infectious or resistant) with replicas outer and nodes inner, in one or
+ * more chunks of whole lines (about 64 MB each); the device formats the
+ * next chunk while the callback handles the current one.  Needs
+ * record_node_states.  Replaces the node rows of write_simulation_state
+ * (tool/gpu_cpu_temporal_sim.cu:505-568). */
+typedef int (*rp_text_cb)(void *user, int32_t step_index, int64_t timestamp,
+                          const char *text, size_t len);
+RP_API rp_status rp_sim_run_text(rp_sim *s, int32_t *counts, rp_text_cb cb,
+                                 void *user);
+
 /* Device-resident replay on a CUDA stream (cudaStream_t, or NULL for the
  * legacy stream): re-initialises the state and enqueues every step; counts
  * stay on the device (rp_sim_counts copies them).  No host synchronisation. */

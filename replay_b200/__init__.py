@@ -246,6 +246,18 @@ class Simulation:
                 "probe_steps": r.probe_steps, "probes": r.probes, "ms_default": r.ms_default,
                 "ms_tuned": r.ms_tuned}
 
+    def run_text(self, write):
+        """Runs the replay with node-state CSV lines formatted on the GPU;
+        write(step_index, timestamp, data: bytes) receives them in chunks of
+        whole lines (requires record_node_states=True).  Returns counts."""
+        counts = self._zeros()
+
+        def _cb(user, step_index, ts, text, n):
+            return int(bool(write(step_index, ts, C.string_at(text, n))))
+        cb = _lib.TEXT_CB(_cb)
+        check(lib().rp_sim_run_text(self._h, _ptr(counts), cb, None))
+        return self._shape(counts)
+
     def profile(self):
         """Device time per kernel group of one eager replay (CUDA events)."""
         pr = _lib.Profile()

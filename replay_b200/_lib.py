@@ -80,6 +80,8 @@ class TuneResult(C.Structure):
                 ("ms_tuned", C.c_double)]
 
 
+TEXT_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_char), C.c_size_t)
+
 SIGNATURES = {
     "rp_last_error": ([], C.c_char_p),
     "rp_version": ([], C.c_char_p),
@@ -104,6 +106,7 @@ SIGNATURES = {
     "rp_sim_free": ([C.c_void_p], None),
     "rp_sim_autotune": ([C.c_void_p, C.c_int32, C.POINTER(TuneResult)], C.c_int),
     "rp_sim_run": ([C.c_void_p, C.c_void_p, STATE_CB, C.c_void_p], C.c_int),
+    "rp_sim_run_text": ([C.c_void_p, C.c_void_p, TEXT_CB, C.c_void_p], C.c_int),
     "rp_sim_enqueue": ([C.c_void_p, C.c_void_p], C.c_int),
     "rp_sim_counts": ([C.c_void_p, C.c_void_p], C.c_int),
     "rp_sim_timestamps": ([C.c_void_p, C.c_void_p], C.c_int),

@@ -43,40 +43,13 @@ static char *fmt_i64(char *p, int64_t v) {
   return p;
 }
 
-static const char *kStateName[4] = {"susceptible", "incubating", "infectious", "resistant"};
-
-static int node_cb(void *user, int32_t step_index, int64_t ts, const uint8_t *states,
-                   int32_t n_nodes, int32_t n_replicas) {
+/* Node-state lines arrive formatted by the device (rp_sim_run_text). */
+static int node_text_cb(void *user, int32_t step_index, int64_t ts, const char *text, size_t len) {
   (void)user;
   (void)step_index;
+  (void)ts;
   if (!g_node_fp) return 0;
-  size_t cap = 1 << 22;
-  char *buf = (char *)malloc(cap);
-  if (!buf) return 1;
-  char *p = buf;
-  for (int32_t r = 0; r < n_replicas; ++r) {
-    for (int32_t i = 0; i < n_nodes; ++i) {
-      if ((size_t)(p - buf) + 80 > cap) {
-        fwrite(buf, 1, (size_t)(p - buf), g_node_fp);
-        p = buf;
-      }
-      p = fmt_i64(p, ts);
-      *p++ = ',';
-      p = fmt_i64(p, r);
-      *p++ = ',';
-      p = fmt_i64(p, i);
-      *p++ = ',';
-      const char *s = kStateName[states[(int64_t)r * n_nodes + i] & 3];
-      size_t L = strlen(s);
-      memcpy(p, s, L);
-      p += L;
-      *p++ = '\n';
-    }
-  }
-  fwrite(buf, 1, (size_t)(p - buf), g_node_fp);
-  free(buf);
-  fflush(g_node_fp);
-  return 0;
+  return fwrite(text, 1, len, g_node_fp) == len ? 0 : 1;
 }
 
 static void usage(const char *argv0) {
@@ -248,7 +221,9 @@ int main(int argc, char **argv) {
     fprintf(stderr, "Error: unable to allocate host arrays.\n");
     return 1;
   }
-  if (rp_sim_run(s, counts, g_node_fp ? node_cb : NULL, NULL) != RP_OK) {
+  const rp_status run_st = g_node_fp ? rp_sim_run_text(s, counts, node_text_cb, NULL)
+                                     : rp_sim_run(s, counts, NULL, NULL);
+  if (run_st != RP_OK) {
     fprintf(stderr, "Error: %s\n", rp_last_error());
     return 1;
   }

@@ -139,6 +139,15 @@ struct rp_sim {
   std::vector<int32_t> h_first, h_rows;  // per network: first row, rows
   std::vector<int32_t> task_rows;        // per network: rows of one task
   int32_t n_slices = 1;
+  // node-state text mode (rp_sim_run_text)
+  rp_text_cb text_cb = nullptr;
+  void *text_user = nullptr;
+  int32_t text_rows = 0;  // replica rows per text chunk
+  int64_t node_digits = 0;
+  DevBuf text_dev[2], text_rowlen, text_rowoff;
+  char *text_host[2] = {nullptr, nullptr};
+  int64_t *text_len_host = nullptr;
+  cudaEvent_t text_ev[2] = {nullptr, nullptr};
   // shared
   DevBuf counts, beta_r, sus, classes;
   StepConsts c{};
@@ -149,7 +158,52 @@ struct rp_sim {
 
   ~rp_sim() {
     if (exec) cudaGraphExecDestroy(exec);
+    if (stream) cudaStreamSynchronize(stream);
+    for (int b = 0; b < 2; ++b) {
+      if (text_host[b]) cudaFreeHost(text_host[b]);
+      if (text_ev[b]) cudaEventDestroy(text_ev[b]);
+    }
+    if (text_len_host) cudaFreeHost(text_len_host);
     if (stream) cudaStreamDestroy(stream);
+  }
+
+  // Node-state CSV lines of one recorded step, formatted on the device in
+  // chunks of replica rows; the host callback writes chunk k while the
+  // device formats chunk k+1.
+  rp_status emit_text(cudaStream_t st, int32_t step_index, int64_t ts) {
+    int prev = -1;
+    int64_t prev_len = 0;
+    for (int32_t r0 = 0, k = 0; r0 < M; r0 += text_rows, ++k) {
+      const int32_t r1 = std::min(M, r0 + text_rows);
+      const int b = k & 1;
+      enqueue_states_text(classes.as<uint8_t>(), N, r0, r1, ts, node_digits,
+                          text_rowlen.as<int64_t>(), text_rowoff.as<int64_t>(),
+                          text_dev[b].as<char>(), st);
+      RP_TRY_CUDA(cudaMemcpyAsync(text_len_host + b, text_rowoff.as<int64_t>() + (r1 - r0),
+                                  sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+      if (prev >= 0) {
+        RP_TRY_CUDA(cudaEventSynchronize(text_ev[prev]));
+        if (text_cb(text_user, step_index, ts, text_host[prev], (size_t)prev_len) != 0) {
+          set_error("text callback aborted the run");
+          return RP_ERR_ARG;
+        }
+      }
+      RP_TRY_CUDA(cudaStreamSynchronize(st));
+      const int64_t len = text_len_host[b];
+      RP_TRY_CUDA(cudaMemcpyAsync(text_host[b], text_dev[b].ptr, (size_t)len,
+                                  cudaMemcpyDeviceToHost, st));
+      RP_TRY_CUDA(cudaEventRecord(text_ev[b], st));
+      prev = b;
+      prev_len = len;
+    }
+    if (prev >= 0) {
+      RP_TRY_CUDA(cudaEventSynchronize(text_ev[prev]));
+      if (text_cb(text_user, step_index, ts, text_host[prev], (size_t)prev_len) != 0) {
+        set_error("text callback aborted the run");
+        return RP_ERR_ARG;
+      }
+    }
+    return RP_OK;
   }
 
   const int32_t *rp_of(int t) const {
@@ -190,13 +244,14 @@ struct rp_sim {
     mark(kMarkStart);
     const int32_t rows = T + 1;
     std::vector<uint8_t> host_states;
-    if (cb) host_states.resize((size_t)N * M);
+    if (cb && !text_cb) host_states.resize((size_t)N * M);
     auto emit_states = [&](int32_t step_index, int64_t tstamp) -> rp_status {
-      if (!cb) return RP_OK;
+      if (!cb && !text_cb) return RP_OK;
       if (path == RP_PATH_BATCHED)
         packed_classify(L, sa.as<uint32_t>(), sb.as<uint32_t>(), classes.as<uint8_t>(), st);
       else
         plain_classify(p.transition, state.ptr, N, M, classes.as<uint8_t>(), c, st);
+      if (text_cb) return emit_text(st, step_index, tstamp);
       RP_TRY_CUDA(cudaMemcpyAsync(host_states.data(), classes.ptr, host_states.size(),
                                   cudaMemcpyDeviceToHost, st));
       RP_TRY_CUDA(cudaStreamSynchronize(st));
@@ -874,6 +929,51 @@ RP_API rp_status rp_sim_run(rp_sim *s, int32_t *counts, rp_state_cb cb, void *us
   } else {
     RP_TRY(s->enqueue(s->stream, nullptr, nullptr, nullptr));
   }
+  RP_TRY_CUDA(cudaMemcpyAsync(counts, s->counts.ptr, s->counts.bytes, cudaMemcpyDeviceToHost,
+                              s->stream));
+  RP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  return RP_OK;
+}
+
+RP_API rp_status rp_sim_run_text(rp_sim *s, int32_t *counts, rp_text_cb cb, void *user) {
+  if (!s || !counts || !cb) {
+    set_error("null argument");
+    return RP_ERR_ARG;
+  }
+  if (!s->p.record_node_states) {
+    set_error("rp_sim_run_text needs a simulation created with record_node_states");
+    return RP_ERR_ARG;
+  }
+  RP_TRY_CUDA(cudaSetDevice(s->g->device));
+  if (!s->text_host[0]) {  // chunk buffers: about 64 MB of text per chunk
+    const int64_t line = text_line_bound(s->N);
+    const int64_t per_row = line * (int64_t)s->N;
+    s->text_rows = (int32_t)std::max<int64_t>(1, std::min<int64_t>(s->M, (64ll << 20) / per_row));
+    const size_t bytes = (size_t)(per_row * s->text_rows);
+    for (int b = 0; b < 2; ++b) {
+      RP_TRY(s->text_dev[b].alloc(bytes));
+      RP_TRY_CUDA(cudaMallocHost(&s->text_host[b], bytes));
+      RP_TRY_CUDA(cudaEventCreateWithFlags(&s->text_ev[b], cudaEventDisableTiming));
+    }
+    RP_TRY_CUDA(cudaMallocHost(&s->text_len_host, 2 * sizeof(int64_t)));
+    RP_TRY(s->text_rowlen.alloc(sizeof(int64_t) * (size_t)s->text_rows));
+    RP_TRY(s->text_rowoff.alloc(sizeof(int64_t) * ((size_t)s->text_rows + 1)));
+    int64_t d = 0;
+    for (int64_t i = 0, p10 = 10, nd = 1; i < s->N; ++i) {
+      if (i == p10) {
+        p10 *= 10;
+        ++nd;
+      }
+      d += nd;
+    }
+    s->node_digits = d;
+  }
+  s->text_cb = cb;
+  s->text_user = user;
+  rp_status st = s->enqueue(s->stream, nullptr, nullptr, nullptr);
+  s->text_cb = nullptr;
+  s->text_user = nullptr;
+  RP_TRY(st);
   RP_TRY_CUDA(cudaMemcpyAsync(counts, s->counts.ptr, s->counts.bytes, cudaMemcpyDeviceToHost,
                               s->stream));
   RP_TRY_CUDA(cudaStreamSynchronize(s->stream));

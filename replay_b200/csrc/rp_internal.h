@@ -169,6 +169,12 @@ void mf_adjoint(int32_t n, const int32_t *rp_c, const int2 *ent_c, const float *
                 float *a_out, float *z_out, float *gsus, double *gpart, cudaStream_t st);
 void mf_finish(const double *gpart, int32_t nblk, double *out, cudaStream_t st);
 
+// ---- node-state text (text.cu) ----
+int64_t text_line_bound(int32_t n_nodes);  // bytes of one line at most
+void enqueue_states_text(const uint8_t *cls, int32_t n, int32_t r0, int32_t r1, int64_t ts,
+                         int64_t node_digits, int64_t *rowlen, int64_t *rowoff, char *out,
+                         cudaStream_t st);
+
 // Scan tiles the window builder uses for n_nodes rows.
 int32_t window_scan_tiles(int32_t n_nodes);
 

@@ -8,9 +8,9 @@ seeded input:
   windows.npz          NCLS hit lists (with the nbuf = nlists cap), FP32 CSRs
                        (build_csr_from_intervals) at weight scales 1 and 1/3,
                        and Eigen SpMM exposures, for random networks
-  replay_*.csv         summary CSVs of `replay --cpu-only` in deterministic
-                       settings (every node infected at t0, infect-prob 1, so
-                       rand() never decides an outcome)
+  replay_*.csv         summary and node-state CSVs of `replay --cpu-only` in
+                       deterministic settings (every node infected at t0,
+                       infect-prob 1, so rand() never decides an outcome)
 
 Run:  python tests/golden/make_golden.py
 """
@@ -144,7 +144,9 @@ def replay_fixtures():
     meta = {}
     for name, args in REPLAY_CASES.items():
         out = os.path.join(HERE, f"replay_{name}.csv")
-        full = [graph, "--cpu-only", "-q", "--start-time", net["t0"], "--summary-out", out] + args
+        nodes = os.path.join(HERE, f"replay_{name}_nodes.csv")
+        full = [graph, "--cpu-only", "-q", "--start-time", net["t0"], "--summary-out", out,
+                "--node-state-out", nodes] + args
         r = ref.run_cli(full)
         assert r.returncode == 0, r.stderr
         meta[name] = [str(a) for a in args] + ["--start-time", str(net["t0"])]

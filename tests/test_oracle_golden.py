@@ -149,3 +149,29 @@ def test_window_hits_half_open(oracle, tmp_path):
     ss, se, su, sv, perm, nl = oracle.sorted_index(r["start"], r["end"], r["u"], r["v"])
     counts = [len(oracle.window_hits(ss, se, len(ss), 60 * k, 60 * (k + 1))) for k in range(4)]
     assert counts == [3, 2, 2, 1]
+
+
+STATE_NAMES = ["susceptible", "incubating", "infectious", "resistant"]
+
+
+def format_node_rows(states, times):
+    """Reference node-CSV lines of (T+1, M, N) states (replicas outer)."""
+    out = ["time,simulation_id,node_id,state\n"]
+    for t, ts in enumerate(times):
+        for r in range(states.shape[1]):
+            out.extend(f"{ts},{r},{i},{STATE_NAMES[s]}\n" for i, s in enumerate(states[t, r]))
+    return "".join(out)
+
+
+@pytest.mark.parametrize("name", ["seirs", "sis_fractional_step", "no_infection"])
+def test_countdown_node_states_match_reference_csv(oracle, golden_dir, name):
+    with open(os.path.join(golden_dir, "replay_cases.json")) as f:
+        kw = cli_args_to_params(json.load(f)[name])
+    got = oracle.parse_file(os.path.join(golden_dir, "replay_graph.txt"))
+    _, states = oracle.run(got["start"], got["end"], got["u"], got["v"], got["n_nodes"], transition=0, seed=5,
+                           node_states=True, **kw)
+    T = kw["n_steps"]
+    ws, we, sc, ts = oracle.schedule(kw["start_time"], kw.get("step_size", 3600.0), kw.get("window", 3600), T)
+    text = format_node_rows(states, [kw["start_time"]] + list(ts))
+    with open(os.path.join(golden_dir, f"replay_{name}_nodes.csv")) as f:
+        assert text == f.read()
