@@ -274,11 +274,39 @@ def run_ours(args, rank, world, local_rank):
         assert counts.shape == (T + 1, M, 4)
         # ---- CPU baseline: the C oracle on a bounded sample ----
         out["cpu_baseline"] = cpu_baseline(net, p)
+        # ---- node-state CSV text formatted on the device ----
+        out["node_state_text"] = node_text_leg(replay_b200, dev)
         # ---- uneven batch of independent networks, default and tuned tiles ----
         out["uneven_batch"] = uneven_batch_leg(replay_b200, dev, timed)
         # ---- expected-value replay: forward, adjoint, beta calibration ----
         out["meanfield"] = meanfield_leg(replay_b200, g, net, p, nnz_total, hbm)
     return out
+
+
+def node_text_leg(replay_b200, dev):
+    """--node-state-out text of the small SEIR replay (N=1,000, 50,000
+    contacts, 168 steps, 1,000 replicas: 169e6 lines) formatted on the
+    device and handed to a callback that only counts the bytes."""
+    from replay_b200 import synthetic
+    net = synthetic.small_seir()
+    g = replay_b200.Graph.from_arrays(net["start"], net["end"], net["u"], net["v"], net["n_nodes"], device=dev)
+    sim = replay_b200.Simulation(g, record_node_states=True, **net["params"])
+    nbytes = [0]
+
+    def count(k, ts, data):
+        nbytes[0] += len(data)
+        return 0
+
+    sim.run_text(count)  # warm-up (buffers)
+    nbytes[0] = 0
+    t0 = time.perf_counter()
+    sim.run_text(count)
+    dt = time.perf_counter() - t0
+    sim.close()
+    g.close()
+    return {"workload": "small SEIR replay, N=1,000 x M=1,000 x 169 recorded steps", "bytes": nbytes[0],
+            "seconds": dt, "GBps": nbytes[0] / dt / 1e9,
+            "includes": "replay + per-step classification + device formatting + D2H into pinned buffers"}
 
 
 def uneven_batch_leg(replay_b200, dev, timed):

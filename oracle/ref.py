@@ -13,6 +13,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(_HERE, "_ref")
 REPLAY_REF = os.path.join(REF_DIR, "replay_ref")
+CONTACT_NETWORK_REF = os.path.join(REF_DIR, "contact_network_ref")
 _LIB = None
 
 i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
