@@ -274,12 +274,58 @@ def run_ours(args, rank, world, local_rank):
         assert counts.shape == (T + 1, M, 4)
         # ---- CPU baseline: the C oracle on a bounded sample ----
         out["cpu_baseline"] = cpu_baseline(net, p)
+        # ---- the reference's own benchmark scenario, both executables ----
+        out["reference_scenario"] = reference_scenario_leg(replay_b200)
         # ---- node-state CSV text formatted on the device ----
         out["node_state_text"] = node_text_leg(replay_b200, dev)
         # ---- uneven batch of independent networks, default and tuned tiles ----
         out["uneven_batch"] = uneven_batch_leg(replay_b200, dev, timed)
         # ---- expected-value replay: forward, adjoint, beta calibration ----
         out["meanfield"] = meanfield_leg(replay_b200, g, net, p, nnz_total, hbm)
+    return out
+
+
+def reference_scenario_leg(replay_b200, reps=3):
+    """The reference's benchmark scenario "villages", population 1,000,
+    trial 1 (benchmark/benchmark_with_trials.py: 100 one-hour steps, group
+    multiplier 0.1, prob_inner 0.9, prob_inter 0.05, 10,000 replicas,
+    initial infected 0.5, infect prob 1.0, E = I = 3600 s, R = 0), its
+    contact file regenerated byte-identically by contact_network; the whole
+    `replay` process is timed end to end (parse, index, 100 steps, no CSV
+    output), as the reference's benchmark times it, for this build and for
+    the reference's GPU path built from its sources, on this GPU."""
+    import hashlib
+    from oracle import ref
+    gen = os.path.join(os.path.dirname(replay_b200.CLI_PATH), "contact_network")
+    env = dict(os.environ, TZ="UTC")
+    seed = int(hashlib.sha256(b"villages_1000_1").hexdigest(), 16) % (10 ** 8)
+    out = {"scenario": "villages, N=1,000, trial 1, 100 x 1 h, M=10,000 (countdown)",
+           "published_reference_gpu_wall_s": [5.71, 5.74], "published_hardware": "not stated"}
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "villages_1000_trial1.txt")
+        subprocess.run([gen, "2000-01-01T00:00:00", "100", "3600", "1000", "100", "0.9", "0.05", path, str(seed)],
+                       env=env, stdout=subprocess.DEVNULL, check=True)
+        with open(path) as f:
+            out["contacts"] = sum(1 for _ in f) - 1
+        args = ["--step-size", "3600.0", "--iterations", "100", "--M", "10000", "--initial-infected", "0.5",
+                "--infect-prob", "1.0", "--exposed-duration", "3600", "--infectious-duration", "3600",
+                "--resistant-duration", "0", "--start-time", "946684800", "--time-step", "3600", "-q"]
+
+        def wall(cmd):
+            times = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                r = subprocess.run(cmd, env=env, capture_output=True)
+                times.append(time.perf_counter() - t0)
+                if r.returncode:
+                    return None
+            return statistics.median(times)
+
+        out["ours_wall_s"] = wall([replay_b200.CLI_PATH, path] + args)
+        if os.path.exists(ref.REPLAY_REF):
+            out["reference_gpu_wall_s"] = wall([ref.REPLAY_REF, path] + args)
+            if out["ours_wall_s"] and out["reference_gpu_wall_s"]:
+                out["speedup_same_gpu"] = out["reference_gpu_wall_s"] / out["ours_wall_s"]
     return out
 
 
