@@ -124,6 +124,12 @@ struct rp_sim {
   std::vector<WinDesc> wins;
   std::vector<CandRange> ranges;
   WindowWorkspace wsp;
+  // per-step mode: window w + 1 is built on a side stream into the other
+  // workspace while window w's steps run
+  WindowWorkspace wsp2;
+  bool overlap = false;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_built[2] = {nullptr, nullptr}, ev_free = nullptr, ev_join = nullptr;
   bool prebuilt = false;
   std::vector<int64_t> arena_rp_off, arena_ent_off;
   DevBuf arena_rp, arena_ent;
@@ -159,6 +165,12 @@ struct rp_sim {
   ~rp_sim() {
     if (exec) cudaGraphExecDestroy(exec);
     if (stream) cudaStreamSynchronize(stream);
+    if (side) {
+      cudaStreamSynchronize(side);
+      cudaStreamDestroy(side);
+    }
+    for (cudaEvent_t e : {ev_built[0], ev_built[1], ev_free, ev_join})
+      if (e) cudaEventDestroy(e);
     for (int b = 0; b < 2; ++b) {
       if (text_host[b]) cudaFreeHost(text_host[b]);
       if (text_ev[b]) cudaEventDestroy(text_ev[b]);
@@ -206,13 +218,15 @@ struct rp_sim {
     return RP_OK;
   }
 
+  WindowWorkspace &ws_of(int w) { return overlap && (w & 1) ? wsp2 : wsp; }
+  const WindowWorkspace &ws_of(int w) const { return overlap && (w & 1) ? wsp2 : wsp; }
   const int32_t *rp_of(int t) const {
     if (prebuilt) return arena_rp.as<int32_t>() + arena_rp_off[step_win[t]];
-    return wsp.row_ptr.as<int32_t>();
+    return ws_of(step_win[t]).row_ptr.as<int32_t>();
   }
   const int2 *ent_of(int t) const {
     if (prebuilt) return arena_ent.as<int2>() + arena_ent_off[step_win[t]];
-    return wsp.entries.as<int2>();
+    return ws_of(step_win[t]).entries.as<int2>();
   }
 
   // Optional event marks around kernel groups (rp_sim_profile).
@@ -282,14 +296,36 @@ struct rp_sim {
     mark(kMarkOther);
     RP_TRY(emit_states(0, p.start_time));
     const int per_row = n_nets * M;
+    const int n_win = (int)wins.size();
+    auto build = [&](int w, cudaStream_t bs) {
+      enqueue_window_build(*g, ws_of(w), w, wins[w], cap, weight_kind,
+                           weight_kind == kWeightF32, bs);
+      // k_hits, k_scan_tiles, k_scan_apply, k_fill (+ k_trunc, + the two row sorts)
+      k += 4 + (wins[w].may_truncate ? 1 : 0) + (weight_kind == kWeightF32 ? 2 : 0);
+    };
+    bool side_used = false;
+    if (!prebuilt && overlap && T > 0) {
+      build(step_win[0], st);
+      mark(kMarkBuild);
+    }
     for (int32_t t = 0; t < T; ++t) {
       const int w = step_win[t];
       if (!prebuilt && (t == 0 || w != step_win[t - 1])) {
-        enqueue_window_build(*g, wsp, w, wins[w], cap, weight_kind,
-                             weight_kind == kWeightF32, st);
-        // k_hits, k_scan_tiles, k_scan_apply, k_fill (+ k_trunc, + the two row sorts)
-        k += 4 + (wins[w].may_truncate ? 1 : 0) + (weight_kind == kWeightF32 ? 2 : 0);
-        mark(kMarkBuild);
+        if (!overlap) {
+          build(w, st);
+          mark(kMarkBuild);
+        } else {
+          if (t > 0) RP_TRY_CUDA(cudaStreamWaitEvent(st, ev_built[w & 1], 0));
+          if (w + 1 < n_win) {
+            // window w-1's steps, the last users of the other workspace, are
+            // all enqueued before this point
+            RP_TRY_CUDA(cudaEventRecord(ev_free, st));
+            RP_TRY_CUDA(cudaStreamWaitEvent(side, ev_free, 0));
+            build(w + 1, side);
+            RP_TRY_CUDA(cudaEventRecord(ev_built[(w + 1) & 1], side));
+            side_used = true;
+          }
+        }
       }
       if (path == RP_PATH_PLAIN) {
         plain_spmv(p.transition, rp_of(t), ent_of(t), state.ptr, exposure.ptr, N, M, c, st);
@@ -314,6 +350,10 @@ struct rp_sim {
         k += 2;
       }
       RP_TRY(emit_states(t + 1, step_ts[t]));
+    }
+    if (side_used) {  // join the side stream (required to end a capture)
+      RP_TRY_CUDA(cudaEventRecord(ev_join, side));
+      RP_TRY_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
     }
     if (path == RP_PATH_BATCHED) {
       packed_finalize_events(init_counts.as<unsigned long long>(),
@@ -873,7 +913,18 @@ RP_API rp_status rp_sim_create_batch(const rp_graph *h, const rp_params *p,
   RP_TRY(sim_setup(*s, h->g, *p));
   RP_TRY(alloc_state(*s));
   s->prebuilt = p->csr_mode == RP_CSR_PREBUILT;
-  if (s->prebuilt) RP_TRY(prebuild(*s));
+  if (s->prebuilt) {
+    RP_TRY(prebuild(*s));
+  } else if (s->wins.size() > 1) {
+    int64_t max_cand = 0;
+    for (const WinDesc &d : s->wins) max_cand = std::max(max_cand, d.n_candidates);
+    RP_TRY(window_workspace_alloc(s->wsp2, s->N, max_cand, (int64_t)s->wins.size(), s->wins,
+                                  s->ranges));
+    RP_TRY_CUDA(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&s->ev_built[0], &s->ev_built[1], &s->ev_free, &s->ev_join})
+      RP_TRY_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    s->overlap = true;
+  }
   for (int32_t t = 0; t < s->T; ++t) {
     // nnz multiplied per step (for the roofline); per-step mode counts the
     // candidate bound, replaced by exact values when prebuilt.
