@@ -114,24 +114,33 @@ struct InfectQueue {
   float efmax[kInfectQueue];     // ef(e_max) of the row
   uint32_t C[32];      // candidates after the bound test (round scratch)
   uint32_t pl[32][4];  // first 4 random planes of each word
-  uint32_t ev[32];     // infection events of each word
   int32_t off[32];     // warp scan offsets of the candidates
   uint8_t have[32];    // planes kept (0 or 4)
+  // candidates carried to the next round (fewer than 32), self-contained
+  uint32_t kpl[32][4];
+  int32_t krloc[32];
+  int32_t kwb[32];  // word << 5 | replica bit
+  uint8_t khave[32];
   int32_t n;
+  int32_t nk;
 };
 
 constexpr int kInfectDynSmem = kEntCap * 8 + 128 * 32 * 4 + kWarps * (int)sizeof(InfectQueue);
 
 // Decides up to 32 queued exposed words: the bound test one word per lane
 // (phase 2), then the exact test of the surviving candidates one replica
-// per lane (phase 3); writes each word's events and flags its item.
-__device__ __forceinline__ void infect_round(InfectQueue &Q, int n, int lane, const PackedLayout &L,
-                                             const PackedTask &T, int cbase, const int32_t *s_rp,
-                                             const int2 *s_ent, const int2 *__restrict__ ent,
-                                             bool staged, int32_t e0, const float *s_beta,
-                                             const float *s_bw, const uint32_t *mask_w,
-                                             uint32_t *evs_w, uint32_t *flag32, uint32_t step,
-                                             float scale, const StepConsts &c) {
+// per lane (phase 3), in full batches of 32 together with the candidates
+// carried from earlier rounds; fewer than 32 left over are carried to the
+// next round unless `drain` is set.  Events are OR-ed into their words and
+// flag their items.
+__device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, int lane,
+                                             const PackedLayout &L, const PackedTask &T,
+                                             int cbase, const int32_t *s_rp, const int2 *s_ent,
+                                             const int2 *__restrict__ ent, bool staged,
+                                             int32_t e0, const float *s_beta, const float *s_bw,
+                                             const uint32_t *mask_w, uint32_t *evs_w,
+                                             uint32_t *flag32, uint32_t step, float scale,
+                                             const StepConsts &c) {
   // ---- phase 2: bound test, one word per lane ----
   uint32_t Cw = 0;
   if (lane < n) {
@@ -156,17 +165,38 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, int lane, co
     }
   }
   Q.C[lane] = Cw;
-  Q.ev[lane] = 0;
   int ctotal;
   Q.off[lane] = warp_excl_scan(__popc(Cw), lane, ctotal);
   __syncwarp();
   // ---- phase 3: exact test, one candidate replica per lane ----
-  for (int p = lane; p < ctotal; p += 32) {
-    const int o = find_owner(Q.off, p);
-    const int b = nth_set_bit(Q.C[o], p - Q.off[o]);
-    const int orl = Q.rloc[o];
+  const int nk = Q.nk;
+  const int total = nk + ctotal;
+  int base = 0;
+  for (; total - base >= 32 || (drain && base < total); base += 32) {
+    const int p = base + lane;
+    if (p >= total) continue;
+    int orl, word, b, have;
+    uint32_t pl[8];
+    if (p < nk) {
+      const int wb = Q.kwb[p];
+      orl = Q.krloc[p];
+      word = wb >> 5;
+      b = wb & 31;
+      have = Q.khave[p];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) pl[q] = Q.kpl[p][q];
+    } else {
+      const int o = find_owner(Q.off, p - nk);
+      b = nth_set_bit(Q.C[o], p - nk - Q.off[o]);
+      orl = Q.rloc[o];
+      word = Q.word[o];
+      have = Q.have[o];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) pl[q] = Q.pl[o][q];
+    }
+#pragma unroll
+    for (int q = 4; q < 8; ++q) pl[q] = 0;
     const int orow = T.row_begin + orl;
-    const int word = Q.word[o];
     long long e = 0;
     const int32_t ob = s_rp[orl], oe = s_rp[orl + 1];
     for (int32_t k = ob; k < oe; ++k) {
@@ -178,29 +208,34 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, int lane, co
     float ef = __ll2float_rn(e);
     if (scale != 1.0f) ef = __fmul_rn(ef, scale);
     const float xx = __fmul_rn(bs, ef);
-    uint32_t pl[8];
-    const int have = Q.have[o];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) pl[q] = Q.pl[o][q];
-#pragma unroll
-    for (int q = 4; q < 8; ++q) pl[q] = 0;
     // P <= x: a uniform at or above x cannot infect (no exponential)
     if (xx > 0.0f && xx < 1.0f &&
         !sliced_less_one((uint32_t)b, fixed64(xx), pl, have, c.rk, (uint32_t)orow, step,
                          (uint32_t)word + (c.roff >> 5), kTagInfect))
       continue;
     if (infect_event(one_minus_exp_neg(xx), pl, have, c.rk, (uint32_t)orow, step,
-                     (uint32_t)word + (c.roff >> 5), (uint32_t)b))
-      atomicOr(&Q.ev[o], 1u << b);
+                     (uint32_t)word + (c.roff >> 5), (uint32_t)b)) {
+      atomicOr(&evs_w[(int64_t)orow * L.words + word], 1u << b);
+      const int64_t idx = (int64_t)orow * L.q4 + (word >> 2);
+      atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
+    }
   }
   __syncwarp();
-  if (lane < n && Q.ev[lane]) {
-    const int64_t row = T.row_begin + Q.rloc[lane];
-    const int word = Q.word[lane];
-    evs_w[row * L.words + word] = Q.ev[lane];
-    const int64_t idx = row * L.q4 + (word >> 2);
-    atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
+  // carry the rest: slots below nk keep their entries when no batch ran
+  const int rest = total - base;
+  if (rest > 0) {
+    const int p = base + lane;
+    if (p < total && p >= nk) {
+      const int o = find_owner(Q.off, p - nk);
+      Q.kwb[lane] = Q.word[o] << 5 | nth_set_bit(Q.C[o], p - nk - Q.off[o]);
+      Q.krloc[lane] = Q.rloc[o];
+      Q.khave[lane] = Q.have[o];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) Q.kpl[lane][q] = Q.pl[o][q];
+    }
   }
+  __syncwarp();
+  if (lane == 0) Q.nk = rest > 0 ? rest : 0;
   __syncwarp();
 }
 
@@ -224,7 +259,10 @@ __global__ void __launch_bounds__(kThreads, 3)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t *mask_w = reinterpret_cast<const uint32_t *>(mask_in);
   uint32_t *evs_w = reinterpret_cast<uint32_t *>(evs);
-  if (lane == 0) Q.n = 0;
+  if (lane == 0) {
+    Q.n = 0;
+    Q.nk = 0;
+  }
   __syncwarp();
   for (int ti = blockIdx.x; ti < L.n_tasks; ti += gridDim.x) {
     const PackedTask T = tasks[ti];
@@ -321,11 +359,12 @@ __global__ void __launch_bounds__(kThreads, 3)
           if (lane == 0) Q.n = base + __popc(qm);
           __syncwarp();
         }
-        // ---- decide full rounds (and, past the items, the remainder) ----
-        while (Q.n >= 32 || (flushing && Q.n > 0)) {
+        // ---- decide full rounds (and, past the items, the remainder and
+        // the carried candidates: the staged pairs change with the chunk) ----
+        while (Q.n >= 32 || (flushing && (Q.n > 0 || Q.nk > 0))) {
           const int take = Q.n < 32 ? Q.n : 32;
-          infect_round(Q, take, lane, L, T, cbase, s_rp, s_ent, ent, staged, e0, s_beta, s_bw,
-                       mask_w, evs_w, flag32, step, scale, c);
+          infect_round(Q, take, flushing && take == Q.n, lane, L, T, cbase, s_rp, s_ent, ent,
+                       staged, e0, s_beta, s_bw, mask_w, evs_w, flag32, step, scale, c);
           const int rest = Q.n - take;
           for (int i = lane; i < rest; i += 32) {
             Q.rloc[i] = Q.rloc[take + i];
