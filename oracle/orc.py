@@ -55,6 +55,8 @@ def lib():
         L.orc_unit.restype = C.c_float
         L.orc_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
         L.orc_uniform.restype = C.c_float
+        L.orc_infect_event.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float]
+        L.orc_infect_event.restype = C.c_int
         L.orc_one_minus_exp_neg.argtypes = [C.c_float]
         L.orc_one_minus_exp_neg.restype = C.c_float
         L.orc_timegm.argtypes = [C.c_int] * 6
@@ -100,6 +102,11 @@ def philox(ctr, key):
 
 def uniform(seed, node, step, replica, stream=0):
     return lib().orc_uniform(seed, node, step, replica, stream)
+
+
+def infect_event(seed, node, step, replica, P):
+    """Geometric-mode infection decision of a replica (orc_infect_event)."""
+    return bool(lib().orc_infect_event(seed, node, step, replica, float(P)))
 
 
 def one_minus_exp_neg(x):

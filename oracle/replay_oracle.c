@@ -110,34 +110,39 @@ int orc_flow_event(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica
   return 0;
 }
 
-/* Bit-sliced comparison U_r < T over 64 bits: bit k of U_r (k = 0 is 2^-1)
- * is bit (r % 32) of output k % 4 of Philox(key = seed, counter = (node,
- * step, r / 32, tag | (k / 4) << 4)). */
-static int sliced_less(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica,
-                       uint32_t tag, uint64_t T) {
+/* Geometric infection uniform U_r of replica r (64 bits, k = 0 is 2^-1)
+ * compared with T = floor(P 2^64): its top 8 bits are bit-sliced -- bit k is
+ * bit (r % 32) of output k % 4 of Philox(key = seed, counter = (node, step,
+ * r / 32, 4 | (k / 4) << 4)), k < 8 -- and its low 56 bits are the top 56
+ * bits of outputs 0-1 (output 0 high) of Philox(counter = (node, step, r,
+ * 12)). */
+static int infect_less(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica,
+                       uint64_t T) {
   uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
   const uint32_t bit = replica & 31u;
-  for (int j = 0; j < 16; j++) {
-    uint32_t ctr[4] = {node, step, replica >> 5, tag | ((uint32_t)j << 4)};
+  uint32_t u8 = 0;
+  for (int j = 0; j < 2; j++) {
+    uint32_t ctr[4] = {node, step, replica >> 5, 4u | ((uint32_t)j << 4)};
     uint32_t x[4];
     orc_philox4x32_10(ctr, key, x);
-    for (int q = 0; q < 4; q++) {
-      const int k = 4 * j + q;
-      const uint32_t wb = (x[q] >> bit) & 1u;
-      const uint32_t tb = (uint32_t)(T >> (63 - k)) & 1u;
-      if (wb != tb) return wb < tb;
-    }
+    for (int q = 0; q < 4; q++) u8 = (u8 << 1) | ((x[q] >> bit) & 1u);
   }
-  return 0;
+  const uint32_t t8 = (uint32_t)(T >> 56);
+  if (u8 != t8) return u8 < t8;
+  uint32_t ctr[4] = {node, step, replica, 12u};
+  uint32_t x[4];
+  orc_philox4x32_10(ctr, key, x);
+  const uint64_t low = (((uint64_t)x[0] << 32) | x[1]) >> 8;
+  return low < (T & 0x00FFFFFFFFFFFFFFull);
 }
 
-/* Infection decision of replica r (geometric mode): its per-step uniform is
- * bit-sliced on tag 4; event iff U_r < floor(P 2^64); P >= 1 always
- * infects, P <= 0 (or NaN) never. */
+/* Infection decision of replica r (geometric mode): event iff
+ * U_r < floor(P 2^64) (infect_less); P >= 1 always infects, P <= 0 (or NaN)
+ * never. */
 int orc_infect_event(uint64_t seed, uint32_t node, uint32_t step, uint32_t replica, float P) {
   if (!(P > 0.0f)) return 0;
   if (P >= 1.0f) return 1;
-  return sliced_less(seed, node, step, replica, 4u, (uint64_t)ldexp((double)P, 64));
+  return infect_less(seed, node, step, replica, (uint64_t)ldexp((double)P, 64));
 }
 
 /* 1 - exp(-x) for x >= 0 using only correctly rounded +,-,*: Cody-Waite

@@ -24,8 +24,9 @@ extern "C" {
  * key = seed; counter = (node, step, c2, c3):
  *   countdown infection uniform of replica r: c2 = r / 4, c3 = 3, output
  *     r % 4, as the 24-bit grid value ((x >> 8) + 1) 2^-24; event iff P > u;
- *   geometric infection uniform: bit-sliced on tag 4 (orc_infect_event),
- *     event iff U < floor(P 2^64);
+ *   geometric infection uniform of replica r: top 8 bits bit-sliced on
+ *     c2 = r / 32, c3 = 4 | j << 4, low 56 bits on c2 = r, c3 = 12
+ *     (orc_infect_event); event iff U < floor(P 2^64);
  *   flow (E->I, I->R, R->S) uniform of replica r: bit-sliced, see
  *     orc_flow_event;
  *   initial Bernoulli: step = 0xFFFFFFFF, c2 = r / 4, c3 = 1;

@@ -15,13 +15,15 @@
 // over 4-word columns (the replacement of cusparseSpMM,
 // tool/gpu_cpu_temporal_sim.cu:1062, and monte_carlo_simulation, :137-159):
 //   1. inf = OR over neighbours j of mask_t[j] (16 B per lane per entry);
-//   2. exposed = inf & S; the exposed replicas of a word compare their
-//      bit-sliced infection uniforms with the word bound B = max bs_r *
-//      e_max (e_max = the row's total contact-seconds, so every P <= B), 32
-//      replicas per random plane; only replicas below B compute their exact
-//      int64 exposure and P = 1 - exp(-beta_r s_i e) and finish the
-//      comparison against floor(P 2^64) (infect_event);
-//   3. events go to evs and the item's flag.
+//   2. exposed = inf & S; the exposed replicas of a word compare the top
+//      byte of their infection uniforms (8 bit-sliced planes, two Philox
+//      calls per word) with that of the word bound B = max bs_r * e_max
+//      (e_max = the row's total contact-seconds, so every P <= B); only
+//      replicas at or below it compute their exact int64 exposure and
+//      P = 1 - exp(-beta_r s_i e) and finish the comparison against
+//      floor(P 2^64) (infect_event; the uniform's low 56 bits are drawn
+//      only on a tie of the top byte);
+//   3. events are OR-ed into evs and flag their item.
 // k_flow (transitions + count reduction), every (row, 4-word column):
 //   reads the planes and the row's infection events, draws the bit-sliced
 //   flow uniforms of the E, I (and waning R) replicas, 32 replicas per random
@@ -108,24 +110,29 @@ constexpr int kEntCap = 1024;       // staged CSR pairs per chunk
 // entries accumulate over rows and are decided 32 at a time.
 constexpr int kInfectQueue = 160;  // 31 left over + 4 words x 32 lanes of one pass
 struct InfectQueue {
+  uint4 pl[32][2];               // the 8 random planes of each word (round scratch)
   int32_t rloc[kInfectQueue];    // task-relative row
   int32_t word[kInfectQueue];    // word index within the row
   uint32_t X[kInfectQueue];      // exposed replicas of the word
   float efmax[kInfectQueue];     // ef(e_max) of the row
   uint32_t C[32];      // candidates after the bound test (round scratch)
-  uint32_t pl[32][4];  // first 4 random planes of each word
   int32_t off[32];     // warp scan offsets of the candidates
-  uint8_t have[32];    // planes kept (0 or 4)
   // candidates carried to the next round (fewer than 32), self-contained
-  uint32_t kpl[32][4];
   int32_t krloc[32];
   int32_t kwb[32];  // word << 5 | replica bit
-  uint8_t khave[32];
+  uint8_t ku8[32];  // top 8 bits of the replica's uniform
   int32_t n;
   int32_t nk;
 };
 
 constexpr int kInfectDynSmem = kEntCap * 8 + 128 * 32 * 4 + kWarps * (int)sizeof(InfectQueue);
+
+// Top 8 uniform bits of replica bit b from a queued word's planes.
+__device__ __forceinline__ uint32_t queued_top8(const uint4 (&q)[2], uint32_t b) {
+  const uint4 a = q[0], c = q[1];
+  const uint32_t pl[8] = {a.x, a.y, a.z, a.w, c.x, c.y, c.z, c.w};
+  return top8_of(pl, b);
+}
 
 // Decides up to 32 queued exposed words: the bound test one word per lane
 // (phase 2), then the exact test of the surviving candidates one replica
@@ -146,22 +153,17 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
   if (lane < n) {
     const int orow = T.row_begin + Q.rloc[lane];
     const int word = Q.word[lane];
-    // every exposed replica has P <= x <= |bs_r| ef(e_max) =: B
+    // every exposed replica has P <= x <= |bs_r| ef(e_max) =: B; replicas
+    // whose uniform's top byte is above B's cannot infect
     float bsmax = c.beta_r ? s_bw[word - 4 * cbase] : fabsf(c.beta);
     if (c.sus) bsmax = __fmul_rn(bsmax, fabsf(c.sus[orow]));
     const float B = __fmul_rn(bsmax, Q.efmax[lane]);
-    uint32_t pl[8];
-    int have = 0;
-    if (B >= 1.0f) {
-      Cw = Q.X[lane];
-    } else if (B > 0.0f) {
-      Cw = sliced_less_word(Q.X[lane], fixed64(B), c.rk, (uint32_t)orow, step,
-                            (uint32_t)word + (c.roff >> 5), kTagInfect, pl, have);
-    }
-    Q.have[lane] = (uint8_t)(have >= 4 ? 4 : 0);
-    if (have >= 4) {
-#pragma unroll
-      for (int q = 0; q < 4; ++q) Q.pl[lane][q] = pl[q];
+    if (B > 0.0f) {
+      uint32_t pl[8];
+      infect_planes(c.rk, (uint32_t)orow, step, (uint32_t)word + (c.roff >> 5), pl);
+      Cw = B >= 1.0f ? Q.X[lane] : top8_le(Q.X[lane], fixed64(B), pl);
+      Q.pl[lane][0] = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+      Q.pl[lane][1] = make_uint4(pl[4], pl[5], pl[6], pl[7]);
     }
   }
   Q.C[lane] = Cw;
@@ -175,27 +177,21 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
   for (; total - base >= 32 || (drain && base < total); base += 32) {
     const int p = base + lane;
     if (p >= total) continue;
-    int orl, word, b, have;
-    uint32_t pl[8];
+    int orl, word, b;
+    uint32_t u8;
     if (p < nk) {
       const int wb = Q.kwb[p];
       orl = Q.krloc[p];
       word = wb >> 5;
       b = wb & 31;
-      have = Q.khave[p];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) pl[q] = Q.kpl[p][q];
+      u8 = Q.ku8[p];
     } else {
       const int o = find_owner(Q.off, p - nk);
       b = nth_set_bit(Q.C[o], p - nk - Q.off[o]);
       orl = Q.rloc[o];
       word = Q.word[o];
-      have = Q.have[o];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) pl[q] = Q.pl[o][q];
+      u8 = queued_top8(Q.pl[o], (uint32_t)b);
     }
-#pragma unroll
-    for (int q = 4; q < 8; ++q) pl[q] = 0;
     const int orow = T.row_begin + orl;
     long long e = 0;
     const int32_t ob = s_rp[orl], oe = s_rp[orl + 1];
@@ -208,13 +204,13 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
     float ef = __ll2float_rn(e);
     if (scale != 1.0f) ef = __fmul_rn(ef, scale);
     const float xx = __fmul_rn(bs, ef);
-    // P <= x: a uniform at or above x cannot infect (no exponential)
-    if (xx > 0.0f && xx < 1.0f &&
-        !sliced_less_one((uint32_t)b, fixed64(xx), pl, have, c.rk, (uint32_t)orow, step,
-                         (uint32_t)word + (c.roff >> 5), kTagInfect))
-      continue;
-    if (infect_event(one_minus_exp_neg(xx), pl, have, c.rk, (uint32_t)orow, step,
-                     (uint32_t)word + (c.roff >> 5), (uint32_t)b)) {
+    if (!(xx > 0.0f)) continue;
+    // P <= x: a uniform whose top byte is above x's cannot infect (no
+    // exponential)
+    if (xx < 1.0f && u8 > (uint32_t)(fixed64(xx) >> 56)) continue;
+    const uint32_t gword = (uint32_t)word + (c.roff >> 5);
+    if (infect_event(one_minus_exp_neg(xx), u8, c.rk, (uint32_t)orow, step,
+                     gword * 32u + (uint32_t)b)) {
       atomicOr(&evs_w[(int64_t)orow * L.words + word], 1u << b);
       const int64_t idx = (int64_t)orow * L.q4 + (word >> 2);
       atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
@@ -227,11 +223,10 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
     const int p = base + lane;
     if (p < total && p >= nk) {
       const int o = find_owner(Q.off, p - nk);
-      Q.kwb[lane] = Q.word[o] << 5 | nth_set_bit(Q.C[o], p - nk - Q.off[o]);
+      const int b = nth_set_bit(Q.C[o], p - nk - Q.off[o]);
+      Q.kwb[lane] = Q.word[o] << 5 | b;
       Q.krloc[lane] = Q.rloc[o];
-      Q.khave[lane] = Q.have[o];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) Q.kpl[lane][q] = Q.pl[o][q];
+      Q.ku8[lane] = (uint8_t)queued_top8(Q.pl[o], (uint32_t)b);
     }
   }
   __syncwarp();

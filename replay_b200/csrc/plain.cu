@@ -183,7 +183,8 @@ __global__ void __launch_bounds__(256)
       }
     }
     const uint32_t word = (uint32_t)(q >> 3) + (c.roff >> 5);  // stream word of the replicas
-    const uint32_t no_planes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t pl[8];  // the word's infection planes, drawn once if needed
+    bool have_pl = false;
     const uint32_t ev = (Em | Im | Rm)
                             ? flow_events(Em, Im, Rm, c.th, c.rk, (uint32_t)i, step, word)
                             : 0u;
@@ -196,7 +197,12 @@ __global__ void __launch_bounds__(256)
       if (v[c4] == 0) {
         if (e[c4] > 0) {
           const float P = one_minus_exp_neg(infection_x(c, r, i, e[c4], scale));
-          if (infect_event(P, no_planes, 0, c.rk, (uint32_t)i, step, word, (uint32_t)(r & 31)))
+          if (P > 0.0f && P < 1.0f && !have_pl) {
+            infect_planes(c.rk, (uint32_t)i, step, word, pl);
+            have_pl = true;
+          }
+          const uint32_t u8 = have_pl ? top8_of(pl, (uint32_t)(r & 31)) : 0u;
+          if (infect_event(P, u8, c.rk, (uint32_t)i, step, word * 32u + (uint32_t)(r & 31)))
             nv = c.has_exposed ? 1 : 2;
         }
       } else if (v[c4] == 1) {

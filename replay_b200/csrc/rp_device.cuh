@@ -67,12 +67,15 @@ __device__ __forceinline__ float unit24(uint32_t x) {
 }
 
 // Random stream layout, key = seed, counter = (node, step, c2, c3):
-//  * infection (S->E / S->I) uniform of replica r: c2 = r / 4, c3 = 3,
-//    output r % 4 on the 24-bit grid; event iff P > u;
+//  * countdown-mode infection (S->E / S->I) uniform of replica r:
+//    c2 = r / 4, c3 = 3, output r % 4 on the 24-bit grid; event iff P > u;
 //  * flow (E->I, I->R, R->S) uniform of replica r: bit-sliced -- bit k of
 //    U_r (k = 0 is 2^-1) is bit r % 32 of output k % 4 of counter
 //    (node, step, r / 32, (k / 4) << 4); event iff U_r < floor(p 2^64)
 //    over the first 64 bits (flow_events);
+//  * geometric-mode infection uniform: top 8 bits bit-sliced on
+//    c3 = 4 | j << 4 (c2 = r / 32), low 56 bits on c2 = r, c3 = 12
+//    (infect_event);
 //  * Bernoulli initial condition: step 0xFFFFFFFF, c2 = r / 4, c3 = 1;
 //  * exact-count initial condition (Floyd): node = draw j, step
 //    0xFFFFFFFE, c2 = r, c3 = 2 (+ 4 x network index).
@@ -158,76 +161,64 @@ __device__ __forceinline__ unsigned long long fixed64(float p) {
   return __float2ull_rz(__fmul_rn(p, 0x1p64f));
 }
 
-// Bit-sliced comparison of the uniforms of the replicas in `cand` (one
-// 32-replica word) with one 64-bit threshold: bit k of U_r is bit r of
-// output k % 4 of counter (node, step, word, tag | (k / 4) << 4).  Returns
-// the replicas with U_r < T; the first 8 planes are kept in pl (*have of
-// them generated) for follow-up comparisons.
-__device__ __forceinline__ uint32_t sliced_less_word(uint32_t cand, unsigned long long T,
-                                                     const uint32_t *rk, uint32_t node,
-                                                     uint32_t step, uint32_t word, uint32_t tag,
-                                                     uint32_t pl[8], int &have) {
-  uint32_t lt = 0, und = cand;
-  have = 0;
-  for (int j = 0; j < 16 && (j < 2 || und != 0u); ++j) {
-    uint32_t x[4];
-    philox4x32_10_rk(node, step, word, tag | ((uint32_t)j << 4), rk, x);
-    if (j == 0) {
-      pl[0] = x[0]; pl[1] = x[1]; pl[2] = x[2]; pl[3] = x[3];
-      have = 4;
-    } else if (j == 1) {
-      pl[4] = x[0]; pl[5] = x[1]; pl[6] = x[2]; pl[7] = x[3];
-      have = 8;
-    }
-    const uint32_t chunk = (uint32_t)(T >> (60 - 4 * j)) & 0xFu;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const uint32_t t = ((chunk >> (3 - q)) & 1u) ? 0xFFFFFFFFu : 0u;
-      const uint32_t w = x[q];
-      lt |= und & t & ~w;
-      und &= ~(t ^ w);
-    }
-  }
-  return lt;
-}
-
-// The 4 bits of replica bit b in planes x[0..3], most significant first.
-__device__ __forceinline__ uint32_t nibble_of(const uint32_t *x, uint32_t b) {
-  return (((x[0] >> b) & 1u) << 3) | (((x[1] >> b) & 1u) << 2) | (((x[2] >> b) & 1u) << 1) |
-         ((x[3] >> b) & 1u);
-}
-
-// U_b < Pf for one replica bit b of the word, first from the kept planes,
-// then from fresh ones; four bits of U and of Pf are compared at a time
-// (the first differing bit decides, as in the plane-by-plane comparison).
-__device__ __forceinline__ bool sliced_less_one(uint32_t b, unsigned long long Pf,
-                                                const uint32_t pl[8], int have,
-                                                const uint32_t *rk, uint32_t node, uint32_t step,
-                                                uint32_t word, uint32_t tag) {
-  for (int j = 0; j < have / 4; ++j) {
-    const uint32_t u4 = nibble_of(pl + 4 * j, b);
-    const uint32_t t4 = (uint32_t)(Pf >> (60 - 4 * j)) & 0xFu;
-    if (u4 != t4) return u4 < t4;
-  }
-  for (int j = have / 4; j < 16; ++j) {
-    uint32_t x[4];
-    philox4x32_10_rk(node, step, word, tag | ((uint32_t)j << 4), rk, x);
-    const uint32_t u4 = nibble_of(x, b);
-    const uint32_t t4 = (uint32_t)(Pf >> (60 - 4 * j)) & 0xFu;
-    if (u4 != t4) return u4 < t4;
-  }
-  return false;
-}
-
-// Geometric infection decision of replica bit b: its uniform is bit-sliced
-// on tag 4; event iff U < floor(P 2^64) (P >= 1 always, P <= 0 or NaN never).
+// Geometric infection uniform U_r of replica r, 64 bits, compared with
+// floor(P 2^64).  Its top 8 bits are bit-sliced: bit k (k = 0 is 2^-1) is bit
+// r % 32 of output k % 4 of counter (node, step, r / 32, 4 | (k / 4) << 4),
+// so that two calls screen all 32 replicas of a word at once.  Its low 56
+// bits are the top 56 bits of outputs 0-1 (output 0 high) of counter
+// (node, step, r, 12), drawn only when the top 8 bits tie with the
+// threshold's.
 constexpr uint32_t kTagInfect = 4u;
-__device__ __forceinline__ bool infect_event(float P, const uint32_t pl[8], int have,
-                                             const uint32_t *rk, uint32_t node, uint32_t step,
-                                             uint32_t word, uint32_t b) {
+constexpr uint32_t kTagInfectTail = 12u;
+
+// The 8 planes of a word's infection uniforms.
+__device__ __forceinline__ void infect_planes(const uint32_t *rk, uint32_t node, uint32_t step,
+                                              uint32_t word, uint32_t pl[8]) {
+  philox4x32_10_rk(node, step, word, kTagInfect, rk, pl);
+  philox4x32_10_rk(node, step, word, kTagInfect | 16u, rk, pl + 4);
+}
+
+// Top 8 bits of the uniform of replica bit b from its word's planes.
+__device__ __forceinline__ uint32_t top8_of(const uint32_t pl[8], uint32_t b) {
+  uint32_t u = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) u = (u << 1) | ((pl[k] >> b) & 1u);
+  return u;
+}
+
+// Replicas of `cand` whose top 8 uniform bits are at most T's: a superset of
+// those with U < T.
+__device__ __forceinline__ uint32_t top8_le(uint32_t cand, unsigned long long T,
+                                            const uint32_t pl[8]) {
+  const uint32_t t8 = (uint32_t)(T >> 56);
+  uint32_t lt = 0, und = cand;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t t = ((t8 >> (7 - k)) & 1u) ? 0xFFFFFFFFu : 0u;
+    lt |= und & t & ~pl[k];
+    und &= ~(t ^ pl[k]);
+  }
+  return lt | und;
+}
+
+// Low 56 bits of the infection uniform of (global) replica `replica`.
+__device__ __forceinline__ unsigned long long infect_tail56(const uint32_t *rk, uint32_t node,
+                                                            uint32_t step, uint32_t replica) {
+  uint32_t x[4];
+  philox4x32_10_rk(node, step, replica, kTagInfectTail, rk, x);
+  return (((unsigned long long)x[0] << 32) | x[1]) >> 8;
+}
+
+// Infection event of a replica whose uniform's top 8 bits are u8: event iff
+// U < floor(P 2^64); P >= 1 always, P <= 0 or NaN never.
+__device__ __forceinline__ bool infect_event(float P, uint32_t u8, const uint32_t *rk,
+                                             uint32_t node, uint32_t step, uint32_t replica) {
   if (!(P > 0.0f)) return false;
   if (P >= 1.0f) return true;
-  return sliced_less_one(b, fixed64(P), pl, have, rk, node, step, word, kTagInfect);
+  const unsigned long long T = fixed64(P);
+  const uint32_t t8 = (uint32_t)(T >> 56);
+  if (u8 != t8) return u8 < t8;
+  return infect_tail56(rk, node, step, replica) < (T & 0x00FFFFFFFFFFFFFFull);
 }
 
 // Countdown arithmetic of the reference (int op float, truncated back to

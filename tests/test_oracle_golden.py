@@ -36,6 +36,42 @@ def test_philox4x32_10_known_answers(oracle):
         assert oracle.philox(ctr, key) == want
 
 
+def _infection_uniform(oracle, seed, node, step, r):
+    """The 64-bit geometric-mode infection uniform of replica r, restated
+    from the stream layout: top 8 bits bit-sliced (bit r % 32 of the outputs
+    of counters (node, step, r / 32, 4 | j << 4), j = 0, 1), low 56 bits the
+    top 56 of outputs 0-1 of counter (node, step, r, 12)."""
+    key = [seed & 0xFFFFFFFF, seed >> 32]
+    u8 = 0
+    for j in range(2):
+        for x in oracle.philox([node, step, r >> 5, 4 | j << 4], key):
+            u8 = u8 << 1 | (x >> (r & 31)) & 1
+    x = oracle.philox([node, step, r, 12], key)
+    return u8 << 56 | (x[0] << 32 | x[1]) >> 8
+
+
+def test_infection_uniform_layout_and_rate(oracle):
+    rng = np.random.default_rng(3)
+    seed = 0x1234_5678_9ABC_DEF0
+    for _ in range(300):
+        node, step, r = (int(v) for v in rng.integers(0, 2**31, 3))
+        U = _infection_uniform(oracle, seed, node, step, r)
+        # thresholds just around U: the top byte ties, the tail decides
+        for P in (np.nextafter(np.float32(U / 2**64), np.float32(2)),
+                  np.nextafter(np.float32(U / 2**64), np.float32(0)), np.float32(rng.random())):
+            P = float(P)
+            if not 0.0 < P < 1.0:
+                continue
+            assert oracle.infect_event(seed, node, step, r, P) == (U < int(math.ldexp(P, 64))), (node, r, P)
+    assert oracle.infect_event(seed, 1, 2, 3, 1.0) and not oracle.infect_event(seed, 1, 2, 3, 0.0)
+    assert not oracle.infect_event(seed, 1, 2, 3, float("nan"))
+    # event rates, for a P just above a top-byte boundary and a generic one
+    n = 20000
+    for P in (np.float32(3 / 256 + 1e-5), np.float32(0.3)):
+        hits = sum(oracle.infect_event(seed, 7 + i // 4096, 11, i % 4096, float(P)) for i in range(n))
+        assert abs(hits / n - P) < 5 * math.sqrt(P * (1 - P) / n), (P, hits / n)
+
+
 def _f32(x):
     return struct.unpack("f", struct.pack("f", x))[0]
 
