@@ -16,6 +16,7 @@ geometric mode takes transition="geometric", beta, p_ei, p_ir, p_rs.
 Every simulation runs on the GPU; there is no CPU fallback.
 """
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -53,8 +54,11 @@ def parse_contacts(path):
     def take(p, ctype, dtype):
         if n == 0:
             return np.zeros(0, dtype)
-        arr = np.ctypeslib.as_array(C.cast(p, C.POINTER(ctype)), shape=(n,)).astype(dtype)
-        L.rp_free(p)
+        # the array views the library's buffer, which is freed when the
+        # array (and every view of it) is gone
+        arr = np.ctypeslib.as_array(C.cast(p, C.POINTER(ctype)), shape=(n,))
+        assert arr.dtype == dtype
+        weakref.finalize(arr, L.rp_free, p.value)
         return arr
 
     return {"n_nodes": nn.value, "n_index": ni.value, "n_malformed": nm.value,

@@ -74,15 +74,80 @@ int64_t iso8601_slow(const char *s) {
   return utc_seconds(year, month, day, hour, min, sec);
 }
 
-struct Contact {
-  int64_t s, e;
-  int32_t a, b;  // raw ids
+struct IdMap {
+  std::vector<int32_t> keys, vals;
+  std::vector<uint8_t> used;
+  size_t mask = 0, count = 0;
+  explicit IdMap(size_t expect) {
+    size_t cap = 1024;
+    while (cap < 2 * expect + 2) cap <<= 1;
+    keys.resize(cap);
+    vals.resize(cap);
+    used.assign(cap, 0);
+    mask = cap - 1;
+  }
+  static size_t h(int32_t k) {
+    uint64_t x = (uint32_t)k * 0x9E3779B97F4A7C15ull;
+    return (size_t)(x ^ (x >> 31));
+  }
+  void grow() {
+    IdMap big(keys.size());
+    for (size_t i = 0; i < keys.size(); ++i)
+      if (used[i]) big.put(keys[i], vals[i]);
+    *this = std::move(big);
+  }
+  void put(int32_t k, int32_t v) {
+    size_t i = h(k) & mask;
+    while (used[i]) i = (i + 1) & mask;
+    used[i] = 1;
+    keys[i] = k;
+    vals[i] = v;
+    ++count;
+  }
+  int32_t get(int32_t k) const {
+    size_t i = h(k) & mask;
+    while (used[i]) {
+      if (keys[i] == k) return vals[i];
+      i = (i + 1) & mask;
+    }
+    return -1;
+  }
+  int32_t get_or_add(int32_t k) {
+    int32_t v = get(k);
+    if (v >= 0) return v;
+    if (2 * (count + 1) > keys.size()) grow();
+    v = (int32_t)count;
+    put(k, v);
+    return v;
+  }
 };
 
+struct Contact {
+  int64_t s, e;
+  int32_t a, b;  // ids numbered by first appearance within the chunk's range
+};
+
+// One thread's share of the file: its contacts, and the raw ids in the order
+// they first appear there (first[j] is the raw id of local number j), so
+// that the file-wide first-appearance numbering is a merge of the ranges in
+// file order.
 struct ChunkResult {
   std::vector<Contact> contacts;
+  IdMap ids{1024};
+  std::vector<int32_t> first;
   int64_t counted = 0;
   int64_t malformed = 0;
+  int32_t local(int32_t raw) {
+    const size_t before = ids.count;
+    const int32_t j = ids.get_or_add(raw);
+    if (ids.count != before) first.push_back(raw);
+    return j;
+  }
+  void add(int64_t ts, int64_t te, int32_t a, int32_t b) {
+    const int32_t la = local(a);  // a before b: the reference indexes the
+    const int32_t lb = local(b);  // first endpoint first
+    contacts.push_back(Contact{ts, te, la, lb});
+  }
 };
 
 inline bool is_blank(char c) { return c == ' ' || c == '\t'; }
@@ -178,10 +243,11 @@ void slow_chunk(const char *p, size_t len, ChunkResult &r) {
   }
   const int64_t ts = iso8601_slow(s), te = iso8601_slow(e);
   if (ts == -1 || te == -1) return;
-  r.contacts.push_back(Contact{ts, te, a, b});
+  r.add(ts, te, a, b);
 }
 
 void parse_range(const char *p, const char *end, ChunkResult &r) {
+  r.contacts.reserve((size_t)(end - p) / 60 + 16);
   while (p < end) {
     const char *nl = (const char *)memchr(p, '\n', (size_t)(end - p));
     const char *le = nl ? nl + 1 : end;  // line including '\n'
@@ -191,7 +257,7 @@ void parse_range(const char *p, const char *end, ChunkResult &r) {
         Contact c;
         if (fast_line(p, le, c)) {
           r.counted++;
-          if (c.s != -1 && c.e != -1) r.contacts.push_back(c);
+          if (c.s != -1 && c.e != -1) r.add(c.s, c.e, c.a, c.b);
         } else {
           slow_chunk(p, len, r);
         }
@@ -204,63 +270,14 @@ void parse_range(const char *p, const char *end, ChunkResult &r) {
   }
 }
 
-struct IdMap {
-  std::vector<int32_t> keys, vals;
-  std::vector<uint8_t> used;
-  size_t mask = 0, count = 0;
-  explicit IdMap(size_t expect) {
-    size_t cap = 1024;
-    while (cap < 2 * expect + 2) cap <<= 1;
-    keys.resize(cap);
-    vals.resize(cap);
-    used.assign(cap, 0);
-    mask = cap - 1;
-  }
-  static size_t h(int32_t k) {
-    uint64_t x = (uint32_t)k * 0x9E3779B97F4A7C15ull;
-    return (size_t)(x ^ (x >> 31));
-  }
-  void grow() {
-    IdMap big(keys.size());
-    for (size_t i = 0; i < keys.size(); ++i)
-      if (used[i]) big.put(keys[i], vals[i]);
-    *this = std::move(big);
-  }
-  void put(int32_t k, int32_t v) {
-    size_t i = h(k) & mask;
-    while (used[i]) i = (i + 1) & mask;
-    used[i] = 1;
-    keys[i] = k;
-    vals[i] = v;
-    ++count;
-  }
-  int32_t get(int32_t k) const {
-    size_t i = h(k) & mask;
-    while (used[i]) {
-      if (keys[i] == k) return vals[i];
-      i = (i + 1) & mask;
-    }
-    return -1;
-  }
-  int32_t get_or_add(int32_t k) {
-    int32_t v = get(k);
-    if (v >= 0) return v;
-    if (2 * (count + 1) > keys.size()) grow();
-    v = (int32_t)count;
-    put(k, v);
-    return v;
-  }
-};
 
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
-rp_status parse_contact_file(const char *path, int32_t &n_nodes,
-                             int32_t &n_index, int64_t &n_malformed,
-                             std::vector<int64_t> &start,
-                             std::vector<int64_t> &end, std::vector<int32_t> &u,
-                             std::vector<int32_t> &v) {
+rp_status parse_contact_file(const char *path, ParsedContacts &out) {
+  out.release_all();
+  out.n = 0;
   int fd = open(path, O_RDONLY);
   if (fd < 0) {
     set_error("could not open file '%s'", path);
@@ -336,7 +353,8 @@ rp_status parse_contact_file(const char *path, int32_t &n_nodes,
     set_error("NODE_LIST too long");
     return RP_ERR_RANGE;
   }
-  n_nodes = (int32_t)ids.size();
+  const int32_t n_nodes = (int32_t)ids.size();
+  out.n_nodes = n_nodes;
 
   // ---- contact lines (the header's own fgets chunks are malformed lines) ----
   int64_t header_chunks = 0;
@@ -364,11 +382,11 @@ rp_status parse_contact_file(const char *path, int32_t &n_nodes,
     for (auto &th : pool) th.join();
   }
   int64_t counted = 0, valid = 0;
-  n_malformed = header_chunks;
+  out.n_malformed = header_chunks;
   for (auto &pr : parts) {
     counted += pr.counted;
     valid += (int64_t)pr.contacts.size();
-    n_malformed += pr.malformed;
+    out.n_malformed += pr.malformed;
   }
   if (counted <= 0) {
     set_error("no valid edge lines found in %s", path);
@@ -388,23 +406,31 @@ rp_status parse_contact_file(const char *path, int32_t &n_nodes,
     return RP_ERR_RANGE;
   }
 
-  // ---- node index: first appearance, sequential over the parts ----
-  IdMap map((size_t)n_nodes);
-  for (auto &pr : parts)
-    for (auto &c : pr.contacts) {
-      map.get_or_add(c.a);
-      map.get_or_add(c.b);
+  // ---- node index: first appearance over the ranges in file order ----
+  std::vector<std::vector<int32_t>> to_global(nthreads);
+  {
+    IdMap map((size_t)n_nodes);
+    for (unsigned t = 0; t < nthreads; ++t) {
+      to_global[t].resize(parts[t].first.size());
+      for (size_t j = 0; j < parts[t].first.size(); ++j)
+        to_global[t][j] = map.get_or_add(parts[t].first[j]);
     }
-  n_index = (int32_t)map.count;
-  if (n_index > n_nodes) {
+    out.n_index = (int32_t)map.count;
+  }
+  if (out.n_index > n_nodes) {
     set_error("contact lines name %d distinct nodes but NODE_LIST declares %d",
-              n_index, n_nodes);
+              out.n_index, n_nodes);
     return RP_ERR_PARSE;
   }
-  start.resize(valid);
-  end.resize(valid);
-  u.resize(valid);
-  v.resize(valid);
+  out.start = (int64_t *)malloc(sizeof(int64_t) * (size_t)valid);
+  out.end = (int64_t *)malloc(sizeof(int64_t) * (size_t)valid);
+  out.u = (int32_t *)malloc(sizeof(int32_t) * (size_t)valid);
+  out.v = (int32_t *)malloc(sizeof(int32_t) * (size_t)valid);
+  if (!out.start || !out.end || !out.u || !out.v) {
+    out.release_all();
+    set_error("out of host memory for %lld contacts", (long long)valid);
+    return RP_ERR_NOMEM;
+  }
   {
     std::vector<int64_t> base(nthreads + 1, 0);
     for (unsigned t = 0; t < nthreads; ++t)
@@ -413,17 +439,20 @@ rp_status parse_contact_file(const char *path, int32_t &n_nodes,
     for (unsigned t = 0; t < nthreads; ++t)
       pool.emplace_back([&, t] {
         int64_t k = base[t];
-        for (auto &c : parts[t].contacts) {
-          const int32_t ia = map.get(c.a), ib = map.get(c.b);
-          start[k] = c.s;
-          end[k] = c.e;
-          u[k] = ia < ib ? ia : ib;
-          v[k] = ia < ib ? ib : ia;
+        const int32_t *g = to_global[t].data();
+        for (const Contact &c : parts[t].contacts) {
+          const int32_t ia = g[c.a], ib = g[c.b];
+          out.start[k] = c.s;
+          out.end[k] = c.e;
+          out.u[k] = ia < ib ? ia : ib;
+          out.v[k] = ia < ib ? ib : ia;
           ++k;
         }
+        std::vector<Contact>().swap(parts[t].contacts);
       });
     for (auto &th : pool) th.join();
   }
+  out.n = valid;
   return RP_OK;
 }
 

@@ -680,16 +680,12 @@ RP_API rp_status rp_graph_load_text(const char *path, int device, rp_graph **out
   }
   *out = nullptr;
   std::unique_ptr<rp_graph> h(new rp_graph());
-  std::vector<int64_t> st, en;
-  std::vector<int32_t> u, v;
-  int32_t n_nodes = 0, n_index = 0;
-  int64_t malformed = 0;
-  RP_TRY(parse_contact_file(path, n_nodes, n_index, malformed, st, en, u, v));
+  ParsedContacts pc;
+  RP_TRY(parse_contact_file(path, pc));
   h->g.device = device;
-  h->g.n_index = n_index;
-  h->g.n_malformed = malformed;
-  RP_TRY(graph_build_device(h->g, st.data(), en.data(), u.data(), v.data(), (int64_t)st.size(),
-                            n_nodes));
+  h->g.n_index = pc.n_index;
+  h->g.n_malformed = pc.n_malformed;
+  RP_TRY(graph_build_device(h->g, pc.start, pc.end, pc.u, pc.v, pc.n, pc.n_nodes));
   *out = h.release();
   return RP_OK;
 }
@@ -704,31 +700,14 @@ RP_API rp_status rp_parse_contacts(const char *path, int32_t *n_nodes, int32_t *
   *start = *end = nullptr;
   *u = *v = nullptr;
   *n_contacts = 0;
-  std::vector<int64_t> st, en;
-  std::vector<int32_t> uu, vv;
-  int32_t nn = 0, ni = 0;
-  int64_t malformed = 0;
-  RP_TRY(parse_contact_file(path, nn, ni, malformed, st, en, uu, vv));
-  *n_nodes = nn;
-  *n_index = ni;
-  *n_malformed = malformed;
-  const size_t n = st.size();
-  if (n == 0) return RP_OK;
-  int64_t *ps = (int64_t *)malloc(n * sizeof(int64_t));
-  int64_t *pe = (int64_t *)malloc(n * sizeof(int64_t));
-  int32_t *pu = (int32_t *)malloc(n * sizeof(int32_t));
-  int32_t *pv = (int32_t *)malloc(n * sizeof(int32_t));
-  if (!ps || !pe || !pu || !pv) {
-    free(ps), free(pe), free(pu), free(pv);
-    set_error("out of host memory for %zu contacts", n);
-    return RP_ERR_NOMEM;
-  }
-  memcpy(ps, st.data(), n * sizeof(int64_t));
-  memcpy(pe, en.data(), n * sizeof(int64_t));
-  memcpy(pu, uu.data(), n * sizeof(int32_t));
-  memcpy(pv, vv.data(), n * sizeof(int32_t));
-  *start = ps, *end = pe, *u = pu, *v = pv;
-  *n_contacts = (int64_t)n;
+  ParsedContacts pc;
+  RP_TRY(parse_contact_file(path, pc));
+  *n_nodes = pc.n_nodes;
+  *n_index = pc.n_index;
+  *n_malformed = pc.n_malformed;
+  *start = pc.start, *end = pc.end, *u = pc.u, *v = pc.v;
+  *n_contacts = pc.n;
+  pc.release();  // the caller frees the arrays with rp_free
   return RP_OK;
 }
 

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <string>
+#include <cstdlib>
 #include <vector>
 
 #include "../../include/replay.h"
@@ -108,11 +109,25 @@ struct Graph {
   DevBuf crank;                    // int32 position in (start asc, end desc) order
 };
 
-rp_status parse_contact_file(const char *path, int32_t &n_nodes,
-                             int32_t &n_index, int64_t &n_malformed,
-                             std::vector<int64_t> &start,
-                             std::vector<int64_t> &end, std::vector<int32_t> &u,
-                             std::vector<int32_t> &v);
+// Contacts read from a text file: malloc'd arrays of n entries in file
+// order (u <= v, compressed indices), owned by this object until release().
+struct ParsedContacts {
+  int32_t n_nodes = 0, n_index = 0;
+  int64_t n_malformed = 0, n = 0;
+  int64_t *start = nullptr, *end = nullptr;
+  int32_t *u = nullptr, *v = nullptr;
+  ParsedContacts() = default;
+  ParsedContacts(const ParsedContacts &) = delete;
+  ParsedContacts &operator=(const ParsedContacts &) = delete;
+  ~ParsedContacts() { release_all(); }
+  void release_all() {
+    free(start), free(end), free(u), free(v);
+    start = end = nullptr;
+    u = v = nullptr;
+  }
+  void release() { start = end = nullptr, u = v = nullptr; }  // ownership passed on
+};
+rp_status parse_contact_file(const char *path, ParsedContacts &out);
 // Builds the device interval index of n contacts given in host memory
 // (u[k] <= v[k]); ingest.cu.
 rp_status graph_build_device(Graph &g, const int64_t *start, const int64_t *end,

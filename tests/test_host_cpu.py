@@ -115,6 +115,45 @@ def test_parser_matches_oracle_on_random_files(oracle, tmp_path, seed, n_lines):
         np.testing.assert_array_equal(got[k], want[k], err_msg=k)
 
 
+def test_parser_first_appearance_across_threads(oracle, tmp_path):
+    """The parser reads a large file in parallel ranges and numbers nodes
+    by first appearance over the whole file.  Here new ids keep appearing
+    down to the last lines (some first as the second endpoint), and lines
+    whose timestamp is rejected (-1, 1969-12-31T23:59:59Z) name ids that no
+    other line does: those must get no number."""
+    rng = np.random.default_rng(11)
+    n_lines, n_ids = 60000, 6000
+    ids = rng.permutation(n_ids) * 7 + 3
+    rejected = np.arange(n_ids, n_ids + 300) * 7 + 3
+    out = ["NODE_LIST " + " ".join(str(int(x)) for x in np.concatenate([ids, rejected])) + "\n"]
+    k_rej = 0
+    for k in range(n_lines):
+        pool = ids[: 2 + (k * n_ids) // n_lines]
+        if k % 200 == 7:
+            out.append(f"{rejected[k_rej]}, {pool[0]}, 1969-12-31T23:59:59Z, 2000-01-01T00:00:00Z;\n")
+            k_rej += 1
+            continue
+        a = int(rng.choice(pool[:-1]))
+        b = int(pool[-1]) if rng.random() < 0.3 else int(rng.choice(pool))
+        if a == b:
+            b = int(pool[0]) if a != pool[0] else int(pool[1])
+        t0 = 946684800 + int(rng.integers(0, 86400 * 20))
+        s = np.datetime64(t0, "s").astype(str) + "Z"
+        e = np.datetime64(t0 + int(rng.integers(1, 3600)), "s").astype(str) + "Z"
+        out.append(f"{a}, {b}, {s}, {e};\n")
+    text = "".join(out)
+    assert len(text) > 2 << 20
+    path = _write(tmp_path, "order", text)
+    got = rb.parse_contacts(path)
+    want = oracle.parse_file(path)
+    assert want["error"] == 0
+    assert got["n_index"] == want["n_index"]
+    assert want["n_index"] > n_ids - 100  # nearly every id is used
+    assert got["n_malformed"] == want["n_malformed"]
+    for k in ("start", "end", "u", "v"):
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+
+
 def test_parser_matches_reference_on_random_files(refshim, tmp_path):
     rng = np.random.default_rng(7)
     path = _write(tmp_path, "ref", random_contact_text(rng, 3000))
