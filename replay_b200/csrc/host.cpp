@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <thread>
 #include <vector>
 
 #include "rp_internal.h"
@@ -681,7 +682,20 @@ RP_API rp_status rp_graph_load_text(const char *path, int device, rp_graph **out
   *out = nullptr;
   std::unique_ptr<rp_graph> h(new rp_graph());
   ParsedContacts pc;
-  RP_TRY(parse_contact_file(path, pc));
+  {
+    // The device's context (a few hundred milliseconds to create, and
+    // needing no input) is created on a helper thread while the file is
+    // parsed; errors surface at the first device call below.
+    struct Joined {
+      std::thread t;
+      ~Joined() {
+        if (t.joinable()) t.join();
+      }
+    } warm{std::thread([device] {
+      if (cudaSetDevice(device) == cudaSuccess) cudaFree(nullptr);
+    })};
+    RP_TRY(parse_contact_file(path, pc));
+  }
   h->g.device = device;
   h->g.n_index = pc.n_index;
   h->g.n_malformed = pc.n_malformed;
