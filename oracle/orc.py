@@ -57,6 +57,10 @@ def lib():
         L.orc_uniform.restype = C.c_float
         L.orc_infect_event.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float]
         L.orc_infect_event.restype = C.c_int
+        L.orc_flow_event.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int]
+        L.orc_flow_event.restype = C.c_int
+        L.orc_threshold64.argtypes = [C.c_float, C.POINTER(C.c_int)]
+        L.orc_threshold64.restype = C.c_uint64
         L.orc_one_minus_exp_neg.argtypes = [C.c_float]
         L.orc_one_minus_exp_neg.restype = C.c_float
         L.orc_timegm.argtypes = [C.c_int] * 6
@@ -107,6 +111,21 @@ def uniform(seed, node, step, replica, stream=0):
 def infect_event(seed, node, step, replica, P):
     """Geometric-mode infection decision of a replica (orc_infect_event)."""
     return bool(lib().orc_infect_event(seed, node, step, replica, float(P)))
+
+
+def flow_event(seed, node, step, replica, p):
+    """Flow decision (E->I, I->R, R->S) of a replica at per-step probability
+    p (orc_threshold64 + orc_flow_event)."""
+    always = C.c_int()
+    T = lib().orc_threshold64(float(p), C.byref(always))
+    return bool(lib().orc_flow_event(seed, node, step, replica, T, always.value))
+
+
+def flow_threshold(p):
+    """floor(p 2^64) for 0 < p < 1 (0 otherwise) and whether p >= 1."""
+    always = C.c_int()
+    T = lib().orc_threshold64(float(p), C.byref(always))
+    return int(T), bool(always.value)
 
 
 def one_minus_exp_neg(x):

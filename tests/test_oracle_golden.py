@@ -72,6 +72,39 @@ def test_infection_uniform_layout_and_rate(oracle):
         assert abs(hits / n - P) < 5 * math.sqrt(P * (1 - P) / n), (P, hits / n)
 
 
+def _flow_uniform(oracle, seed, node, step, r):
+    """The 64-bit flow uniform of replica r, restated from the stream
+    layout: bit k (k = 0 is 2^-1) is bit r % 32 of output k % 4 of counter
+    (node, step, r / 32, (k / 4) << 4)."""
+    key = [seed & 0xFFFFFFFF, seed >> 32]
+    u = 0
+    for j in range(16):
+        for x in oracle.philox([node, step, r >> 5, j << 4], key):
+            u = u << 1 | (x >> (r & 31)) & 1
+    return u
+
+
+def test_flow_uniform_layout_and_rate(oracle):
+    rng = np.random.default_rng(4)
+    seed = 0x0FED_CBA9_8765_4321
+    for _ in range(200):
+        node, step, r = (int(v) for v in rng.integers(0, 2**31, 3))
+        U = _flow_uniform(oracle, seed, node, step, r)
+        for p in (np.nextafter(np.float32(U / 2**64), np.float32(2)),
+                  np.nextafter(np.float32(U / 2**64), np.float32(0)), np.float32(rng.random())):
+            T, always = oracle.flow_threshold(float(p))
+            if always or T == 0:
+                continue
+            assert T == int(math.ldexp(float(p), 64))
+            assert oracle.flow_event(seed, node, step, r, float(p)) == (U < T), (node, r, p)
+    assert oracle.flow_threshold(1.0) == (0, True) and oracle.flow_event(seed, 1, 2, 3, 1.0)
+    assert oracle.flow_threshold(0.0) == (0, False) and not oracle.flow_event(seed, 1, 2, 3, 0.0)
+    n = 20000
+    for p in (np.float32(1 / 48), np.float32(0.5)):
+        hits = sum(oracle.flow_event(seed, 5 + i // 4096, 9, i % 4096, float(p)) for i in range(n))
+        assert abs(hits / n - p) < 5 * math.sqrt(p * (1 - p) / n), (p, hits / n)
+
+
 def _f32(x):
     return struct.unpack("f", struct.pack("f", x))[0]
 
