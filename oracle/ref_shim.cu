@@ -79,9 +79,9 @@ int ref_parse(const char *path, int quiet, int *n_nodes, int64_t **start,
   return count;
 }
 
-// Builds the NCLS over the given contacts and runs the driver's per-step
-// query for [ws, we).  Hit buffers must hold `n` entries.  Returns the number
-// of hits the driver would pass to build_csr_from_intervals.
+// Builds the NCLS over the given contacts and runs the reference main loop's
+// per-step query for [ws, we).  Hit buffers must hold `n` entries.  Returns
+// the number of hits that loop would pass to build_csr_from_intervals.
 int ref_window_query(const int64_t *start, const int64_t *end,
                      const int32_t *src, const int32_t *tgt, int n, int64_t ws,
                      int64_t we, int *out_nlists, int *out_ncompact,

@@ -68,7 +68,7 @@ void orc_sort_order(const int64_t *start, const int64_t *end, int64_t n,
                     int64_t *perm);
 /* nlists of the reference's nested containment list over these contacts. */
 int64_t orc_nlists(const int64_t *start, const int64_t *end, int64_t n);
-/* Window query with the driver's hit cap (max(nlists,1)).  Contacts must be
+/* Window query with the reference main loop's hit cap (max(nlists,1)).  Contacts must be
  * given in stored coordinates and sorted order (orc_sort_order).  Writes sorted positions of hits in
  * query order into out_rank (capacity n).  Returns the hit count. */
 int64_t orc_window_hits(const int64_t *s_start, const int64_t *s_end, int64_t n,

@@ -7,8 +7,8 @@ trajectories cannot be matched one to one.  Both `replay` executables run
 the same countdown SIR configuration on the same contact file with 10,000
 replicas each; the summary CSVs are compared per time point and compartment
 (two-sample z of the means against the 95% interval) and on the final
-epidemic size (two-sample Kolmogorov-Smirnov).  Runs on the GPU box, where
-the reference's GPU path can run; needs the reference built from its
+epidemic size (two-sample Kolmogorov-Smirnov).  Runs where a GPU is present,
+so that the reference's GPU path can run too; needs the reference built from its
 sources (oracle/_ref/replay_ref).
 """
 import os
