@@ -215,8 +215,8 @@ int main(int argc, char **argv) {
          "window: %lld seconds\n",
          (long long)p.start_time, (double)p.step_size, (long long)p.window);
   /* Callers time the simulation phase from the moment this marker arrives
-   * on a pipe (replay/scaling/*_benchmark.py), so it is not left in the
-   * stdio buffer until the end. */
+   * on a pipe (the scaling benchmark scripts under replay/scaling), so it is
+   * not left in the stdio buffer until the end. */
   fflush(stdout);
   const int32_t M = p.n_replicas, T = p.n_steps;
   int32_t *counts = (int32_t *)malloc(sizeof(int32_t) * (size_t)(T + 1) * (size_t)M * 4);
