@@ -16,8 +16,11 @@
 //  * timestamps are "%d-%d-%dT%d:%d:%d" in UTC with timegm's normalisation
 //    of out-of-range fields; a timestamp equal to -1 rejects the line;
 //  * node index = order of first appearance in contact lines.
-// Canonical lines take a hand-written fast path (parallel over threads);
-// every other line goes through sscanf with the reference's two patterns.
+// Lines of the exact form "id, id, YYYY-MM-DDTHH:MM:SSZ, YYYY-MM-DDTHH:MM:SSZ;"
+// (what the network generator writes) are read at fixed offsets; other
+// lines both patterns read alike take a hand-written scanning path; every
+// other line goes through sscanf with the reference's two patterns.  The
+// file is split into one range per thread.
 #include <fcntl.h>
 #include <sys/mman.h>
 #include <sys/stat.h>
@@ -134,13 +137,26 @@ struct Contact {
 struct ChunkResult {
   std::vector<Contact> contacts;
   IdMap ids{1024};
+  std::vector<int32_t> dense;  // local number of raw id i (< dense.size()), -1 if none yet
   std::vector<int32_t> first;
   int64_t counted = 0;
   int64_t malformed = 0;
   int32_t local(int32_t raw) {
-    const size_t before = ids.count;
-    const int32_t j = ids.get_or_add(raw);
-    if (ids.count != before) first.push_back(raw);
+    if ((uint32_t)raw < dense.size()) {
+      int32_t &d = dense[(uint32_t)raw];
+      if (d < 0) {
+        d = (int32_t)first.size();
+        first.push_back(raw);
+      }
+      return d;
+    }
+    int32_t j = ids.get(raw);
+    if (j < 0) {
+      j = (int32_t)first.size();
+      if (2 * (ids.count + 1) > ids.keys.size()) ids.grow();
+      ids.put(raw, j);
+      first.push_back(raw);
+    }
     return j;
   }
   void add(int64_t ts, int64_t te, int32_t a, int32_t b) {
@@ -246,9 +262,70 @@ void slow_chunk(const char *p, size_t len, ChunkResult &r) {
   r.add(ts, te, a, b);
 }
 
+// "DDDD-DD-DDTDD:DD:DDZ" exactly (the generator's and most files' form).
+inline bool canon_ts(const char *p, int64_t &out) {
+  static const char kSep[20] = {0, 0, 0, 0, '-', 0, 0, '-', 0, 0, 'T', 0, 0, ':', 0, 0, ':', 0, 0, 'Z'};
+  uint32_t dg[20];
+  bool ok = true;
+#pragma GCC unroll 20
+  for (int i = 0; i < 20; ++i) {
+    if (kSep[i]) {
+      ok &= p[i] == kSep[i];
+    } else {
+      dg[i] = (uint32_t)(unsigned char)p[i] - (uint32_t)'0';
+      ok &= dg[i] <= 9u;
+    }
+  }
+  if (!ok) return false;
+  out = utc_seconds(dg[0] * 1000 + dg[1] * 100 + dg[2] * 10 + dg[3], dg[5] * 10 + dg[6],
+                    dg[8] * 10 + dg[9], dg[11] * 10 + dg[12], dg[14] * 10 + dg[15],
+                    dg[17] * 10 + dg[18]);
+  return true;
+}
+
+// "id, id, TS, TS;" with ids of 1-9 digits and TS in canon_ts form; returns
+// the position just past ';', or nullptr for any other shape.
+inline const char *canon_line(const char *p, const char *end, Contact &c) {
+  int64_t v[2];
+  for (int k = 0; k < 2; ++k) {
+    int n = 0;
+    int64_t x = 0;
+    while (p < end && is_digit(*p) && n < 10) {
+      x = x * 10 + (*p - '0');
+      ++p;
+      ++n;
+    }
+    if (n == 0 || n > 9 || end - p < 2 || p[0] != ',' || p[1] != ' ') return nullptr;
+    p += 2;
+    v[k] = x;
+  }
+  if (end - p < 43 || p[20] != ',' || p[21] != ' ' || p[42] != ';') return nullptr;
+  int64_t ts, te;
+  if (!canon_ts(p, ts) || !canon_ts(p + 22, te)) return nullptr;
+  c.s = ts;
+  c.e = te;
+  c.a = (int32_t)v[0];
+  c.b = (int32_t)v[1];
+  return p + 43;
+}
+
 void parse_range(const char *p, const char *end, ChunkResult &r) {
   r.contacts.reserve((size_t)(end - p) / 60 + 16);
   while (p < end) {
+    if (*p != '#') {
+      Contact c;
+      const char *q = canon_line(p, end, c);
+      if (q) {
+        const char *nl = (const char *)memchr(q, '\n', (size_t)(end - q));
+        const char *le = nl ? nl + 1 : end;
+        if ((size_t)(le - p) <= kFgetsChunk) {
+          r.counted++;
+          if (c.s != -1 && c.e != -1) r.add(c.s, c.e, c.a, c.b);
+          p = le;
+          continue;
+        }
+      }
+    }
     const char *nl = (const char *)memchr(p, '\n', (size_t)(end - p));
     const char *le = nl ? nl + 1 : end;  // line including '\n'
     const size_t len = (size_t)(le - p);
@@ -375,10 +452,21 @@ rp_status parse_contact_file(const char *path, ParsedContacts &out) {
     cuts[t] = nl ? nl + 1 : body_end;
   }
   std::vector<ChunkResult> parts(nthreads);
+  // ids in [0, max NODE_LIST id] are numbered through a dense table per
+  // thread when all tables together stay within 64M entries (256 MB)
+  size_t dense_n = 0;
+  {
+    long max_id = 0;
+    for (long id : ids) max_id = id > max_id ? id : max_id;
+    if ((size_t)(max_id + 1) * nthreads <= ((size_t)1 << 26)) dense_n = (size_t)max_id + 1;
+  }
   {
     std::vector<std::thread> pool;
     for (unsigned t = 0; t < nthreads; ++t)
-      pool.emplace_back([&, t] { parse_range(cuts[t], cuts[t + 1], parts[t]); });
+      pool.emplace_back([&, t] {
+        parts[t].dense.assign(dense_n, -1);
+        parse_range(cuts[t], cuts[t + 1], parts[t]);
+      });
     for (auto &th : pool) th.join();
   }
   int64_t counted = 0, valid = 0;

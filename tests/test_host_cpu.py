@@ -154,6 +154,49 @@ def test_parser_first_appearance_across_threads(oracle, tmp_path):
         np.testing.assert_array_equal(got[k], want[k], err_msg=k)
 
 
+def _fixed_form_text():
+    lines = [
+        "1, 2, 2000-01-01T00:00:00Z, 2000-01-01T01:00:00Z;\n",
+        "123456789, 2, 2000-01-01T00:00:00Z, 2000-01-01T01:00:00Z;\n",  # 9-digit id, not listed
+        "1234567890, 2, 2000-01-01T00:00:00Z, 2000-01-01T01:00:00Z;\n",  # 10 digits: general rules
+        "3, 4, 2000-13-40T25:61:61Z, 2001-02-30T00:00:00Z;\r\n",  # normalised like timegm
+        "5, 6, 1969-12-31T23:59:59Z, 2000-01-01T00:00:00Z;\n",  # start == -1: rejected
+        "# 7, 8, 2000-01-01T00:00:00Z, 2000-01-01T01:00:00Z;\n",
+        "7,8, 2000-01-01T00:00:00Z, 2000-01-01T01:00:00Z;\n",  # one separator without blank
+        "9, 10, 2000-01-01T00:00:00, 2000-01-01T01:00:00Z;\n",  # no Z on the start
+        "11, 12, 2000-1-01T00:00:00Z, 2000-01-01T01:00:00Z;\n",  # short month field
+        " 13, 14, 2000-01-01T00:00:00Z, 2000-01-01T01:00:00Z;\n",  # leading blank
+        "15, 16, 2000-01-01T00:00:00Z, 2000-01-01T01:00:00Z; trailing\n",
+        "17, 18, 2000-01-01T00:00:00Z, 2000-01-01T01:00:00Z;" + "x" * 150000 + "\n",  # > one chunk
+        "19, 20, 2000-01-01T00:00:00Z, 2000-01-01T01:00:00Z;",  # no final newline
+    ]
+    ids = [1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 123456789, 1234567890]
+    return "NODE_LIST " + " ".join(map(str, ids)) + "\n" + "".join(lines)
+
+
+def test_parser_fixed_form_lines_match_reference(refshim, tmp_path):
+    path = _write(tmp_path, "fixed_ref", _fixed_form_text())
+    got = rb.parse_contacts(path)
+    want = refshim.parse(path)
+    for k in ("start", "end", "u", "v"):
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+
+
+def test_parser_fixed_form_lines_and_their_edges(oracle, tmp_path):
+    """Lines in the generator's exact form take a fixed-offset path; lines
+    that only nearly have that form, and a fixed-form line longer than one
+    fgets chunk (whose tail the reference reads as further lines), must
+    come out as the general rules read them."""
+    path = _write(tmp_path, "fixed", _fixed_form_text())
+    got = rb.parse_contacts(path)
+    want = oracle.parse_file(path)
+    assert want["error"] == 0
+    assert got["n_index"] == want["n_index"] and got["n_malformed"] == want["n_malformed"]
+    for k in ("start", "end", "u", "v"):
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+    assert len(got["start"]) >= 10
+
+
 def test_parser_matches_reference_on_random_files(refshim, tmp_path):
     rng = np.random.default_rng(7)
     path = _write(tmp_path, "ref", random_contact_text(rng, 3000))
