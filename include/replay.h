@@ -127,9 +127,11 @@ RP_API rp_status rp_window_csr(rp_graph *g, int64_t ws, int64_t we,
  * (about 9 MB per device), so the graph may have at most 65,536 nodes and
  * the window at most 131,072 candidate contacts (RP_ERR_RANGE beyond).
  * Calls share that scratch: concurrent or overlapping calls race, so issue
- * them one at a time.  The first call on a device looks the scratch up
- * (cudaGetSymbolAddress); make it before any stream capture.  Returns when
- * the CSR is in place; *nnz and *n_hits as for rp_window_csr. */
+ * them one at a time.  Each call looks the scratch up (cudaGetSymbolAddress),
+ * copies small descriptors from the host and synchronizes `stream` before it
+ * returns, so it must not be made while `stream` is being captured.  The
+ * caller's current device is restored.  Returns when the CSR is in place;
+ * *nnz and *n_hits as for rp_window_csr. */
 RP_API rp_status rp_window_csr_noalloc(rp_graph *g, int64_t ws, int64_t we,
                                        float scale, int32_t weight_kind,
                                        int32_t ncls_cap, int32_t *d_row_ptr,

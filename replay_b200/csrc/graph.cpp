@@ -550,8 +550,8 @@ static int64_t sat_sub(int64_t a, int64_t b) {  // a - b, b >= 0, saturating
   return a - b;
 }
 
-void plan_window(const Graph &g, int64_t ws, int64_t we, float scale,
-                 int64_t cap, std::vector<CandRange> &ranges, WinDesc &out) {
+int32_t plan_window_ranges(const Graph &g, int64_t ws, int64_t we, float scale, int64_t cap,
+                           CandRange *ranges, WinDesc &out) {
   out.ws = ws;
   out.we = we;
   out.scale = scale;
@@ -563,7 +563,7 @@ void plan_window(const Graph &g, int64_t ws, int64_t we, float scale,
     out.qs = ws;
     out.qe = we;
   }
-  out.range_off = (int32_t)ranges.size();
+  out.range_off = 0;
   out.n_ranges = 0;
   out.n_candidates = 0;
   for (int c = 0; c < kClasses; ++c) {
@@ -577,11 +577,19 @@ void plan_window(const Graph &g, int64_t ws, int64_t we, float scale,
     auto hi = std::lower_bound(lo, last, out.qe);
     const int64_t count = hi - lo;
     if (count <= 0) continue;
-    ranges.push_back(CandRange{(int64_t)(lo - g.h_cs.begin()), count, out.n_candidates});
+    ranges[out.n_ranges++] = CandRange{(int64_t)(lo - g.h_cs.begin()), count, out.n_candidates};
     out.n_candidates += count;
-    out.n_ranges++;
   }
   out.may_truncate = out.n_candidates > cap ? 1 : 0;
+  return out.n_ranges;
+}
+
+void plan_window(const Graph &g, int64_t ws, int64_t we, float scale,
+                 int64_t cap, std::vector<CandRange> &ranges, WinDesc &out) {
+  CandRange r[kClasses];
+  const int32_t n = plan_window_ranges(g, ws, we, scale, cap, r, out);
+  out.range_off = (int32_t)ranges.size();
+  ranges.insert(ranges.end(), r, r + n);
 }
 
 }  // namespace rp

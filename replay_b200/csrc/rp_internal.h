@@ -134,6 +134,10 @@ rp_status graph_build_device(Graph &g, const int64_t *start, const int64_t *end,
                              const int32_t *u, const int32_t *v, int64_t n, int32_t n_nodes);
 
 // Plans the query of one window: candidate ranges appended to `ranges`.
+// Candidate ranges of window [ws, we) (at most kClasses, written to `ranges`,
+// range_off = 0); returns their number.  plan_window appends them to a list.
+int32_t plan_window_ranges(const Graph &g, int64_t ws, int64_t we, float scale, int64_t cap,
+                           CandRange *ranges, WinDesc &out);
 void plan_window(const Graph &g, int64_t ws, int64_t we, float scale,
                  int64_t cap, std::vector<CandRange> &ranges, WinDesc &out);
 

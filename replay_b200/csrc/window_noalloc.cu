@@ -13,13 +13,12 @@
 // candidate contacts in one window (contacts whose stored start falls inside
 // the window's scan range); larger requests fail with RP_ERR_RANGE.  The
 // scratch array is shared by all calls on a device, so calls must not
-// overlap: issue them from one thread on one stream at a time.  The first
-// call on each device looks up the array's address (cudaGetSymbolAddress,
-// which may load this module); make that first call before any stream
-// capture begins.
-#include <algorithm>
-#include <atomic>
-
+// overlap: issue them from one thread on one stream at a time.  Every call
+// looks up the array's address (cudaGetSymbolAddress; the first call in a
+// context may load this module), copies small descriptors from the host
+// stack and synchronizes the stream before it returns, so a call cannot be
+// made while the stream is being captured.  The caller's current device is
+// restored on return.
 #include "rp_internal.h"
 
 namespace rp {
@@ -28,7 +27,6 @@ namespace {
 constexpr int32_t kNoAllocMaxNodes = 65536;
 constexpr int64_t kNoAllocMaxCandidates = 131072;
 constexpr int32_t kNoAllocMaxTiles = 64;
-constexpr int kMaxDevices = 64;
 
 constexpr size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -50,50 +48,29 @@ constexpr size_t kScratchBytes = kRangeOff + align256(sizeof(CandRange) * kClass
 
 static __device__ __align__(256) unsigned char g_window_scratch[kScratchBytes];
 
-std::atomic<void *> g_scratch_addr[kMaxDevices];
-
-// Address of the scratch array on `device` (the current device).
-rp_status scratch_address(int device, unsigned char **out) {
-  if (device < 0 || device >= kMaxDevices) {
-    set_error("device %d out of range for the allocation-free window build", device);
-    return RP_ERR_ARG;
-  }
-  void *p = g_scratch_addr[device].load(std::memory_order_acquire);
-  if (!p) {
-    cudaError_t e = cudaGetSymbolAddress(&p, g_window_scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(window scratch)");
-    g_scratch_addr[device].store(p, std::memory_order_release);
-  }
+// Address of the scratch array in the current device's context.  Looked up
+// on every call (no allocation, and cheap): a cached address would go stale
+// if the primary context were reset and the module reloaded elsewhere.
+rp_status scratch_address(unsigned char **out) {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_window_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(window scratch)");
   *out = static_cast<unsigned char *>(p);
   return RP_OK;
 }
 
-// plan_window's candidate ranges written to a fixed array (at most kClasses).
-void plan_window_fixed(const Graph &g, int64_t ws, int64_t we, float scale, int64_t cap,
-                       CandRange *ranges, WinDesc &out) {
-  out.ws = ws;
-  out.we = we;
-  out.scale = scale;
-  out.qs = ws < 0 ? -we : ws;  // mirrored query for a negative start (intervaldb.c:437-444)
-  out.qe = ws < 0 ? -ws : we;
-  out.range_off = 0;
-  out.n_ranges = 0;
-  out.n_candidates = 0;
-  for (int c = 0; c < kClasses; ++c) {
-    const int64_t b0 = g.class_off[c], b1 = g.class_off[c + 1];
-    if (b1 <= b0) continue;
-    const int64_t span = c >= 63 ? INT64_MAX : ((int64_t)1 << c);
-    const int64_t lo_key = out.qs < INT64_MIN + span ? INT64_MIN : out.qs - span;
-    auto first = g.h_cs.begin() + b0, last = g.h_cs.begin() + b1;
-    auto lo = std::upper_bound(first, last, lo_key);
-    auto hi = std::lower_bound(lo, last, out.qe);
-    const int64_t count = hi - lo;
-    if (count <= 0) continue;
-    ranges[out.n_ranges++] = CandRange{(int64_t)(lo - g.h_cs.begin()), count, out.n_candidates};
-    out.n_candidates += count;
+// Makes `device` current for the scope and restores the caller's device.
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DeviceScope(int device) {
+    err = cudaGetDevice(&prev);
+    if (err == cudaSuccess && prev != device) err = cudaSetDevice(device);
   }
-  out.may_truncate = out.n_candidates > cap ? 1 : 0;
-}
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 rp_status window_csr_noalloc(const Graph &g, int64_t ws, int64_t we, float scale, int weight_kind,
                              int ncls_cap, int32_t *d_row_ptr, int32_t *d_entries,
@@ -112,14 +89,15 @@ rp_status window_csr_noalloc(const Graph &g, int64_t ws, int64_t we, float scale
               kNoAllocMaxNodes);
     return RP_ERR_RANGE;
   }
-  RP_TRY_CUDA(cudaSetDevice(g.device));
+  DeviceScope scope(g.device);
+  if (scope.err != cudaSuccess) return cuda_fail(scope.err, "cudaSetDevice");
   unsigned char *base = nullptr;
-  RP_TRY(scratch_address(g.device, &base));
+  RP_TRY(scratch_address(&base));
 
   const int64_t cap = ncls_cap ? (g.nlists > 0 ? g.nlists : 1) : INT64_MAX;
   CandRange ranges[kClasses];
   WinDesc desc{};
-  plan_window_fixed(g, ws, we, scale, cap, ranges, desc);
+  plan_window_ranges(g, ws, we, scale, cap, ranges, desc);
   if (desc.n_candidates > kNoAllocMaxCandidates) {
     set_error("window [%lld, %lld) scans %lld candidate contacts; the allocation-free window "
               "build takes at most %lld", (long long)ws, (long long)we,
