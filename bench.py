@@ -219,21 +219,18 @@ def run_ours(args, rank, world, local_rank):
         out["prebuilt_csr"] = {"value": nrs_per_replay * world / (ms_pre / 1e3), "ms_per_step": ms_pre,
                                "prebuilt_nnz": sim_pre.info["prebuilt_nnz"]}
 
-    # ---- roofline of the step: k_infect + k_flow, one launch each per step ----
+    # ---- roofline of the step: k_step, one launch per step ----
     hbm, peak_kind = load_peaks()
     prof = prof_ps if args.no_extras else sim_pre.profile()
     bytes_replay = algorithmic_bytes(n_nodes, M, T, nnz_total)
-    infect_ms = prof["spmv_ms"] / max(1, prof["spmv_launches"])
-    flow_ms = prof["step_ms"] / max(1, prof["step_launches"])
-    step_launch_ms = infect_ms + flow_ms
+    step_launch_ms = prof["step_ms"] / max(1, prof["step_launches"])
     achieved = (bytes_replay / T) / (step_launch_ms / 1e3) / 1e9
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                        "frac": achieved / hbm, "peak_source": f"{peak_kind} (copy bandwidth)",
-                       "kernel": "k_infect + k_flow (the two launches of one step)",
+                       "kernel": "k_step (one launch per step)",
                        "algorithmic_bytes_per_launch": bytes_replay / T,
                        "avg_launch_us": step_launch_ms * 1e3,
-                       "avg_launch_us_by_kernel": {"k_infect": infect_ms * 1e3, "k_flow": flow_ms * 1e3},
-                       "traffic": profiled_traffic(args.workload)}
+                       "traffic": None}
     out["profile_ms"] = {"per_step": prof} if args.no_extras else {"prebuilt": prof, "per_step": sim.profile()}
 
     if not args.no_extras and rank == 0:

@@ -138,7 +138,8 @@ struct rp_sim {
   // plain state
   DevBuf state, exposure;
   // batched state
-  DevBuf sa, sb, mask, evs, flag, tasks, ev, rs, init_counts;
+  DevBuf sa, sb, mask, mask2, tasks, ev, rs, init_counts;
+  DevBuf err;  // int32: set by a kernel that gave up a bounded wait
   PackedLayout L{};
   DevBuf net_size, net_first, net_rows;
   int32_t n_nets = 1;
@@ -283,12 +284,10 @@ struct rp_sim {
       k += 2 + (p.initial_count > 0);
     } else {
       RP_TRY_CUDA(cudaMemsetAsync(ev.ptr, 0, ev.bytes, st));
-      // k_infect writes event words one by one; k_flow reads whole items
-      RP_TRY_CUDA(cudaMemsetAsync(evs.ptr, 0, evs.bytes, st));
       if (rs.ptr && p.p_rs > 0.0f) RP_TRY_CUDA(cudaMemsetAsync(rs.ptr, 0, rs.bytes, st));
       RP_TRY_CUDA(cudaMemsetAsync(init_counts.ptr, 0, init_counts.bytes, st));
       packed_init(L, sa.as<uint32_t>(), sb.as<uint32_t>(), mask.as<uint32_t>(),
-                  flag.as<uint8_t>(), p.initial_infected, p.initial_count, net_first.as<int32_t>(),
+                  p.initial_infected, p.initial_count, net_first.as<int32_t>(),
                   net_rows.as<int32_t>(), n_nets, c, st);
       packed_count(L, tasks.as<PackedTask>(), sa.as<uint32_t>(), sb.as<uint32_t>(),
                    init_counts.as<unsigned long long>(), st);
@@ -337,18 +336,18 @@ struct rp_sim {
         mark(kMarkStep);
         k += 2;
       } else {
-        packed_infect(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t), mask.as<uint32_t>(),
-                      sa.as<uint32_t>(), sb.as<uint32_t>(), evs.as<uint32_t>(),
-                      flag.as<uint8_t>(), (uint32_t)t, step_scale[t], c, st);
-        mark(kMarkSpmv);
-        packed_flow(L, tasks.as<PackedTask>(), rp_of(t), mask.as<uint32_t>(), sa.as<uint32_t>(),
-                    sb.as<uint32_t>(), evs.as<uint32_t>(), flag.as<uint8_t>(),
-                    ev.as<unsigned long long>() + (int64_t)t * per_row,
-                    p.p_rs > 0.0f ? rs.as<unsigned long long>() + (int64_t)t * per_row
-                                  : nullptr,
-                    (uint32_t)t, c, st);
+        // the infectious masks alternate: step t reads buffer t & 1 and
+        // writes every word of the other
+        const uint32_t *m_in = (t & 1) ? mask2.as<uint32_t>() : mask.as<uint32_t>();
+        uint32_t *m_out = (t & 1) ? mask.as<uint32_t>() : mask2.as<uint32_t>();
+        packed_step_fused(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t), m_in, m_out,
+                          sa.as<uint32_t>(), sb.as<uint32_t>(),
+                          ev.as<unsigned long long>() + (int64_t)t * per_row,
+                          p.p_rs > 0.0f ? rs.as<unsigned long long>() + (int64_t)t * per_row
+                                        : nullptr,
+                          (uint32_t)t, step_scale[t], c, st);
         mark(kMarkStep);
-        k += 2;
+        k += 1;
       }
       RP_TRY(emit_states(t + 1, step_ts[t]));
     }
@@ -418,7 +417,8 @@ rp_status prebuild(rp_sim &s) {
   }
   s.prebuilt_nnz = ent;
   RP_TRY(s.arena_rp.alloc(sizeof(int32_t) * (size_t)nw * ((size_t)N + 1)));
-  RP_TRY(s.arena_ent.alloc(sizeof(int2) * (size_t)(ent > 0 ? ent : 1)));
+  // two spare pairs for the step kernel's 16-byte bulk staging
+  RP_TRY(s.arena_ent.alloc(sizeof(int2) * (size_t)(ent + 2)));
   for (int w = 0; w < nw; ++w) {
     enqueue_window_build(*s.g, s.wsp, w, s.wins[w], s.cap, s.weight_kind, true, st);
     enqueue_window_compact(s.wsp, s.arena_rp.as<int32_t>() + s.arena_rp_off[w],
@@ -584,6 +584,9 @@ rp_status upload_tasks(rp_sim &s) {
 rp_status alloc_state(rp_sim &s) {
   const int32_t N = s.N, M = s.M, T = s.T;
   const int64_t NM = (int64_t)N * M;
+  RP_TRY(s.err.alloc(sizeof(int32_t)));
+  RP_TRY_CUDA(cudaMemset(s.err.ptr, 0, sizeof(int32_t)));
+  s.c.err = s.err.as<int32_t>();
   RP_TRY(s.counts.alloc(sizeof(int32_t) * (size_t)(T + 1) * (size_t)M * 4 * s.n_nets));
   if (s.p.record_node_states) RP_TRY(s.classes.alloc((size_t)NM));
   if (s.path == RP_PATH_PLAIN) {
@@ -624,12 +627,12 @@ rp_status alloc_state(rp_sim &s) {
   // network smaller than a task is one task); rp_sim_autotune refines them
   s.task_rows.assign(s.n_nets, rows_per_task(N, n_slices));
   RP_TRY(packed_prepare());
+  RP_TRY(step_prepare());
   const size_t plane = sizeof(uint32_t) * (size_t)N * L.words;
   RP_TRY(s.sa.alloc(plane));
   RP_TRY(s.sb.alloc(plane));
   RP_TRY(s.mask.alloc(plane));
-  RP_TRY(s.evs.alloc(plane));
-  RP_TRY(s.flag.alloc(((size_t)N * L.q4 + 3) / 4 * 4));
+  RP_TRY(s.mask2.alloc(plane));
   RP_TRY(upload_tasks(s));
   const size_t per_row = (size_t)s.n_nets * M;
   RP_TRY(s.ev.alloc(sizeof(unsigned long long) * per_row * (size_t)(T > 0 ? T : 1)));
@@ -665,6 +668,20 @@ rp_status capture(rp_sim &s) {
 }
 
 }  // namespace
+
+// Fails when a kernel of the last replay gave up a bounded wait (the flag is
+// sticky until read here).
+rp_status check_kernel_flag(rp_sim &s, cudaStream_t st) {
+  int32_t flag = 0;
+  RP_TRY_CUDA(cudaMemcpyAsync(&flag, s.err.ptr, sizeof(flag), cudaMemcpyDeviceToHost, st));
+  RP_TRY_CUDA(cudaStreamSynchronize(st));
+  if (flag) {
+    RP_TRY_CUDA(cudaMemsetAsync(s.err.ptr, 0, sizeof(int32_t), st));
+    set_error("a step kernel gave up waiting for its staged copies; results are invalid");
+    return RP_ERR_DEVICE;
+  }
+  return RP_OK;
+}
 
 // ===========================================================================
 // C ABI
@@ -956,6 +973,7 @@ RP_API rp_status rp_sim_counts(rp_sim *s, int32_t *counts) {
   }
   RP_TRY_CUDA(cudaSetDevice(s->g->device));
   RP_TRY_CUDA(cudaDeviceSynchronize());
+  RP_TRY(check_kernel_flag(*s, s->stream));
   RP_TRY_CUDA(cudaMemcpy(counts, s->counts.ptr, s->counts.bytes, cudaMemcpyDeviceToHost));
   return RP_OK;
 }
@@ -975,7 +993,7 @@ RP_API rp_status rp_sim_run(rp_sim *s, int32_t *counts, rp_state_cb cb, void *us
   }
   RP_TRY_CUDA(cudaMemcpyAsync(counts, s->counts.ptr, s->counts.bytes, cudaMemcpyDeviceToHost,
                               s->stream));
-  RP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  RP_TRY(check_kernel_flag(*s, s->stream));
   return RP_OK;
 }
 
@@ -1020,7 +1038,7 @@ RP_API rp_status rp_sim_run_text(rp_sim *s, int32_t *counts, rp_text_cb cb, void
   RP_TRY(st);
   RP_TRY_CUDA(cudaMemcpyAsync(counts, s->counts.ptr, s->counts.bytes, cudaMemcpyDeviceToHost,
                               s->stream));
-  RP_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  RP_TRY(check_kernel_flag(*s, s->stream));
   return RP_OK;
 }
 
@@ -1049,7 +1067,7 @@ RP_API rp_status rp_sim_get_info(const rp_sim *s, rp_sim_info *o) {
   o->prebuilt_nnz = s->prebuilt_nnz;
   int64_t bytes = 0;
   const DevBuf *bufs[] = {&s->arena_rp, &s->arena_ent, &s->state, &s->exposure, &s->sa,
-                          &s->sb, &s->mask, &s->evs, &s->flag, &s->tasks, &s->ev, &s->rs,
+                          &s->sb, &s->mask, &s->mask2, &s->err, &s->tasks, &s->ev, &s->rs,
                           &s->init_counts, &s->counts, &s->beta_r, &s->sus, &s->classes,
                           &s->wsp.hits, &s->wsp.entries, &s->wsp.erank, &s->wsp.tmp_e,
                           &s->wsp.tmp_r, &s->wsp.row_ptr, &s->wsp.deg, &s->wsp.tiles,

@@ -133,6 +133,7 @@ __device__ __forceinline__ uint32_t flow_events(uint32_t E, uint32_t I, uint32_t
   const uint32_t i2 = (th.ti_all || th.ti == 0) ? 0u : I;
   const uint32_t r2 = (th.tr_all || th.tr == 0) ? 0u : R;
   uint32_t und = e2 | i2 | r2;
+  if (und == 0u) return lt;  // every candidate's threshold is 0 or 1: no draw
   // the first two calls (8 planes) run unconditionally so that lanes stay in
   // step; later planes only while some replica is undecided
   for (int j = 0; j < 16 && (j < 2 || und != 0u); ++j) {

@@ -538,7 +538,9 @@ rp_status window_workspace_alloc(WindowWorkspace &w, int32_t n_nodes,
   w.n_tiles = (int32_t)((n_nodes + kScanTile - 1) / kScanTile);
   if (w.n_tiles < 1) w.n_tiles = 1;
   RP_TRY(w.hits.alloc(sizeof(Hit) * w.cap_hits));
-  RP_TRY(w.entries.alloc(sizeof(int2) * w.cap_entries));
+  // two spare pairs: the step kernel stages entry ranges with 16-byte bulk
+  // copies that may read 8 bytes past the last pair
+  RP_TRY(w.entries.alloc(sizeof(int2) * (w.cap_entries + 2)));
   RP_TRY(w.erank.alloc(sizeof(int32_t) * w.cap_entries));
   RP_TRY(w.tmp_e.alloc(sizeof(int2) * w.cap_entries));
   RP_TRY(w.tmp_r.alloc(sizeof(int32_t) * w.cap_entries));
