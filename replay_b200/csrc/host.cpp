@@ -102,9 +102,73 @@ rp_status make_schedule(const rp_params &p, std::vector<int64_t> &ws,
   return RP_OK;
 }
 
+// Countdown arithmetic of the reference, on the host (IEEE single
+// precision, no contraction): c = (int)((float)c - step), c = (int)((float)base + step).
+int32_t host_cd_sub(int32_t c, float step) { return (int32_t)((float)c - step); }
+int32_t host_cd_add(int32_t base, float step) { return (int32_t)((float)base + step); }
+
+// Summary class of a countdown value (tool/gpu_cpu_temporal_sim.cu:530-550).
+uint32_t host_cd_class(int32_t c, int32_t E, int32_t I, int32_t R) {
+  const int32_t upper = E + I + R;
+  const int32_t elapsed = (c <= 0 || c > upper) ? 0 : (upper - c);
+  if (c == 0) return 0;
+  if (E > 0 && elapsed < E) return 1;
+  if (I > 0 && elapsed < E + I) return 2;
+  if (R > 0 && elapsed < E + I + R) return 3;
+  return 0;
+}
+
+// The countdown values a replica can hold within n_steps steps, as codes
+// (countdown.cu): code 0 is c == 0; the sequence from an infection (base
+// E + I + R) and from an initial infection (base I + R) follow, each cut
+// after n_steps + 2 values.  Entry: next code | class << 16 | infectious << 18.
+struct CdTable {
+  std::vector<uint32_t> tab;
+  uint32_t infect_code = 0;  // code of a replica infected this step, after the step's decrement
+  uint32_t init_code = 0;    // code of an initially infected replica at t0
+  int code_bytes = 0;        // 1 or 2; 0 when the table is too large
+};
+
+void build_cd_table(const rp_params &p, CdTable &t) {
+  const int32_t E = p.exposed_duration, I = p.infectious_duration, R = p.resistant_duration;
+  const int32_t upper = E + I + R, medium = I + R, lower = R;
+  const float step = p.step_size;
+  const int64_t cap = (int64_t)(p.n_steps > 0 ? p.n_steps : 0) + 2;
+  t.tab.assign(1, 0u);  // code 0: susceptible, stays
+  auto entry = [&](int32_t c) {
+    const uint32_t inf = (c > lower && c <= medium) ? 1u : 0u;
+    return host_cd_class(c, E, I, R) << 16 | inf << 18;
+  };
+  auto sequence = [&](int32_t c) -> uint32_t {  // returns the first value's code
+    const uint32_t first = (uint32_t)t.tab.size();
+    for (int64_t k = 0; k < cap && c > 0 && t.tab.size() <= 65536; ++k) {
+      const uint32_t code = (uint32_t)t.tab.size();
+      t.tab.push_back(entry(c));
+      int32_t nx = host_cd_sub(c, step);
+      if (nx < 0) nx = 0;
+      // next code: 0 when the countdown ends, itself at the cut (never
+      // reached within the replay)
+      const uint32_t next = nx == 0 ? 0u : (k + 1 < cap ? code + 1 : code);
+      t.tab.back() |= next & 0xFFFFu;
+      c = nx;
+    }
+    return t.tab.size() > first ? first : 0u;
+  };
+  const int32_t c_inf = host_cd_add(upper, step);
+  const uint32_t inf_first = c_inf > 0 ? sequence(c_inf) : 0u;
+  // the infection's value takes its first decrement in the same step
+  t.infect_code = inf_first ? (t.tab[inf_first] & 0xFFFFu) : 0u;
+  const int32_t c_init = host_cd_add(medium, step);
+  t.init_code = c_init > 0 ? sequence(c_init) : 0u;
+  t.code_bytes = t.tab.size() <= 256 ? 1 : (t.tab.size() <= 65536 ? 2 : 0);
+}
+
 int resolve_path(const rp_params &p) {
   if (p.path != RP_PATH_AUTO) return p.path;
-  return p.transition == RP_TRANSITION_GEOMETRIC ? RP_PATH_BATCHED : RP_PATH_PLAIN;
+  if (p.transition == RP_TRANSITION_GEOMETRIC) return RP_PATH_BATCHED;
+  CdTable t;
+  build_cd_table(p, t);
+  return t.code_bytes ? RP_PATH_BATCHED : RP_PATH_PLAIN;
 }
 
 }  // namespace
@@ -140,6 +204,9 @@ struct rp_sim {
   // batched state
   DevBuf sa, sb, mask, mask2, tasks, ev, rs, init_counts;
   DevBuf err;  // int32: set by a kernel that gave up a bounded wait
+  // batched countdown state: per-replica codes into the countdown table
+  DevBuf codes, cd_tab;
+  CdTable cd;
   PackedLayout L{};
   DevBuf net_size, net_first, net_rows;
   int32_t n_nets = 1;
@@ -263,7 +330,10 @@ struct rp_sim {
     if (cb && !text_cb) host_states.resize((size_t)N * M);
     auto emit_states = [&](int32_t step_index, int64_t tstamp) -> rp_status {
       if (!cb && !text_cb) return RP_OK;
-      if (path == RP_PATH_BATCHED)
+      if (path == RP_PATH_BATCHED && cd.code_bytes)
+        cd_classify(L, codes.ptr, cd.code_bytes, cd_tab.as<uint32_t>(), classes.as<uint8_t>(),
+                    st);
+      else if (path == RP_PATH_BATCHED)
         packed_classify(L, sa.as<uint32_t>(), sb.as<uint32_t>(), classes.as<uint8_t>(), st);
       else
         plain_classify(p.transition, state.ptr, N, M, classes.as<uint8_t>(), c, st);
@@ -289,8 +359,13 @@ struct rp_sim {
       packed_init(L, sa.as<uint32_t>(), sb.as<uint32_t>(), mask.as<uint32_t>(),
                   p.initial_infected, p.initial_count, net_first.as<int32_t>(),
                   net_rows.as<int32_t>(), n_nets, c, st);
-      packed_count(L, tasks.as<PackedTask>(), sa.as<uint32_t>(), sb.as<uint32_t>(),
-                   init_counts.as<unsigned long long>(), st);
+      if (cd.code_bytes)  // countdown codes from the initial-infection plane
+        cd_init(L, tasks.as<PackedTask>(), sa.as<uint32_t>(), codes.ptr, cd.code_bytes,
+                mask.as<uint32_t>(), cd_tab.as<uint32_t>(), cd.init_code,
+                init_counts.as<unsigned long long>(), st);
+      else
+        packed_count(L, tasks.as<PackedTask>(), sa.as<uint32_t>(), sb.as<uint32_t>(),
+                     init_counts.as<unsigned long long>(), st);
       k += 2 + 2 * (p.initial_count > 0);
     }
     mark(kMarkOther);
@@ -340,12 +415,17 @@ struct rp_sim {
         // writes every word of the other
         const uint32_t *m_in = (t & 1) ? mask2.as<uint32_t>() : mask.as<uint32_t>();
         uint32_t *m_out = (t & 1) ? mask.as<uint32_t>() : mask2.as<uint32_t>();
-        packed_step_fused(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t), m_in, m_out,
-                          sa.as<uint32_t>(), sb.as<uint32_t>(),
-                          ev.as<unsigned long long>() + (int64_t)t * per_row,
-                          p.p_rs > 0.0f ? rs.as<unsigned long long>() + (int64_t)t * per_row
-                                        : nullptr,
-                          (uint32_t)t, step_scale[t], c, st);
+        if (cd.code_bytes)
+          cd_step(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t), m_in, m_out, codes.ptr,
+                  cd.code_bytes, cd_tab.as<uint32_t>(), (int32_t)cd.tab.size(), cd.infect_code,
+                  ev.as<unsigned long long>() + (int64_t)t * per_row, (uint32_t)t, c, st);
+        else
+          packed_step_fused(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t), m_in, m_out,
+                            sa.as<uint32_t>(), sb.as<uint32_t>(),
+                            ev.as<unsigned long long>() + (int64_t)t * per_row,
+                            p.p_rs > 0.0f ? rs.as<unsigned long long>() + (int64_t)t * per_row
+                                          : nullptr,
+                            (uint32_t)t, step_scale[t], c, st);
         mark(kMarkStep);
         k += 1;
       }
@@ -355,7 +435,12 @@ struct rp_sim {
       RP_TRY_CUDA(cudaEventRecord(ev_join, side));
       RP_TRY_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
     }
-    if (path == RP_PATH_BATCHED) {
+    if (path == RP_PATH_BATCHED && cd.code_bytes) {
+      cd_finalize(init_counts.as<unsigned long long>(), ev.as<unsigned long long>(), T, per_row,
+                  net_size.as<int32_t>(), M, counts.as<int32_t>(), st);
+      k += 1;
+      mark(kMarkOther);
+    } else if (path == RP_PATH_BATCHED) {
       packed_finalize_events(init_counts.as<unsigned long long>(),
                              ev.as<unsigned long long>(),
                              p.p_rs > 0.0f ? rs.as<unsigned long long>() : nullptr, T,
@@ -448,8 +533,12 @@ rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
     return RP_ERR_ARG;
   }
   if (s.path == RP_PATH_BATCHED && p.transition == RP_TRANSITION_COUNTDOWN) {
-    set_error("countdown transitions run on the plain path");
-    return RP_ERR_ARG;
+    build_cd_table(p, s.cd);
+    if (!s.cd.code_bytes) {
+      set_error("countdown values of this replay need more than 65536 codes; the batched "
+                "path stores at most 65536 (use the plain path)");
+      return RP_ERR_RANGE;
+    }
   }
   if (p.initial_count > s.N) {
     set_error("initial_count %d exceeds the %d nodes", p.initial_count, s.N);
@@ -628,11 +717,18 @@ rp_status alloc_state(rp_sim &s) {
   s.task_rows.assign(s.n_nets, rows_per_task(N, n_slices));
   RP_TRY(packed_prepare());
   RP_TRY(step_prepare());
+  RP_TRY(cd_prepare());
   const size_t plane = sizeof(uint32_t) * (size_t)N * L.words;
   RP_TRY(s.sa.alloc(plane));
   RP_TRY(s.sb.alloc(plane));
   RP_TRY(s.mask.alloc(plane));
   RP_TRY(s.mask2.alloc(plane));
+  if (s.cd.code_bytes) {
+    RP_TRY(s.codes.alloc((size_t)s.cd.code_bytes * 32 * (size_t)N * L.words));
+    RP_TRY(s.cd_tab.alloc(sizeof(uint32_t) * s.cd.tab.size()));
+    RP_TRY_CUDA(cudaMemcpy(s.cd_tab.ptr, s.cd.tab.data(), sizeof(uint32_t) * s.cd.tab.size(),
+                           cudaMemcpyHostToDevice));
+  }
   RP_TRY(upload_tasks(s));
   const size_t per_row = (size_t)s.n_nets * M;
   RP_TRY(s.ev.alloc(sizeof(unsigned long long) * per_row * (size_t)(T > 0 ? T : 1)));
@@ -900,7 +996,7 @@ RP_API rp_status rp_sim_create_batch(const rp_graph *h, const rp_params *p,
     }
     if (n_networks > 1) {
       if (resolve_path(*p) != RP_PATH_BATCHED) {
-        set_error("a multi-network batch runs on the batched (geometric) path");
+        set_error("a multi-network batch runs on the batched path");
         return RP_ERR_ARG;
       }
       if (p->ncls_cap) {
@@ -1067,7 +1163,8 @@ RP_API rp_status rp_sim_get_info(const rp_sim *s, rp_sim_info *o) {
   o->prebuilt_nnz = s->prebuilt_nnz;
   int64_t bytes = 0;
   const DevBuf *bufs[] = {&s->arena_rp, &s->arena_ent, &s->state, &s->exposure, &s->sa,
-                          &s->sb, &s->mask, &s->mask2, &s->err, &s->tasks, &s->ev, &s->rs,
+                          &s->sb, &s->mask, &s->mask2, &s->err, &s->codes, &s->cd_tab,
+                          &s->tasks, &s->ev, &s->rs,
                           &s->init_counts, &s->counts, &s->beta_r, &s->sus, &s->classes,
                           &s->wsp.hits, &s->wsp.entries, &s->wsp.erank, &s->wsp.tmp_e,
                           &s->wsp.tmp_r, &s->wsp.row_ptr, &s->wsp.deg, &s->wsp.tiles,

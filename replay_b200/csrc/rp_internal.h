@@ -273,6 +273,21 @@ void packed_step_fused(const PackedLayout &L, const PackedTask *tasks,
                        uint32_t *sb, unsigned long long *ev_row,
                        unsigned long long *rs_row, uint32_t step, float scale,
                        const StepConsts &c, cudaStream_t st);
+// Batched countdown mode (countdown.cu): per-replica codes into the host's
+// countdown table (next | class << 16 | infectious << 18), 1 or 2 bytes each.
+rp_status cd_prepare();
+void cd_init(const PackedLayout &L, const PackedTask *tasks, const uint32_t *infected,
+             void *codes, int code_bytes, uint32_t *mask, const uint32_t *tab,
+             uint32_t init_code, unsigned long long *init_counts, cudaStream_t st);
+void cd_step(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
+             const int2 *entries, const uint32_t *mask_in, uint32_t *mask_out, void *codes,
+             int code_bytes, const uint32_t *tab, int32_t n_codes, uint32_t infect_code,
+             unsigned long long *ev_row, uint32_t step, const StepConsts &c, cudaStream_t st);
+void cd_finalize(const unsigned long long *init, const unsigned long long *ev, int32_t steps,
+                 int32_t per_row, const int32_t *net_size, int32_t m, int32_t *counts,
+                 cudaStream_t st);
+void cd_classify(const PackedLayout &L, const void *codes, int code_bytes, const uint32_t *tab,
+                 uint8_t *out, cudaStream_t st);
 void packed_count(const PackedLayout &L, const PackedTask *tasks,
                   const uint32_t *sa, const uint32_t *sb,
                   unsigned long long *counts_row, cudaStream_t st);

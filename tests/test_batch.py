@@ -87,7 +87,28 @@ def test_batch_argument_errors():
     with pytest.raises(rb.ReplayError, match="smallest network"):
         rb.Simulation(g, networks=off, initial_count=31, **kw)
     with pytest.raises(rb.ReplayError, match="batched"):
-        rb.Simulation(g, networks=off, **dict(kw, transition="countdown"))
+        rb.Simulation(g, networks=off, **dict(kw, path="plain"))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("csr", ["per-step", "prebuilt"])
+def test_countdown_batch_matches_oracle(oracle, csr):
+    """The reference's countdown rules on a batch of uneven networks."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import replay_b200 as rb
+    nets = _nets(seed=80)
+    s, e, u, v, n, off = _union(nets)
+    kw = dict(M=70, iterations=24, step_size=1800.0, window=1800, start_time=nets[0]["t0"], seed=13,
+              transition="countdown", initial_count=3, infect_prob=0.3, exposed_duration=3600,
+              infectious_duration=7200, resistant_duration=5400)
+    g = rb.Graph.from_arrays(s, e, u, v, n)
+    got = rb.Simulation(g, networks=off, path="batched", csr=csr, **kw).run()
+    okw = {"M": "n_replicas", "iterations": "n_steps"}
+    want = oracle.run(s, e, u, v, n, net_first=off, ncls_cap=0,
+                      **{okw.get(k, k): (0 if k == "transition" else val) for k, val in kw.items()})
+    np.testing.assert_array_equal(got, want)
 
 
 @pytest.mark.gpu

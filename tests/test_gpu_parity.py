@@ -103,17 +103,21 @@ COUNTDOWN_CASES = [
          exposed_duration=0, infectious_duration=5000, resistant_duration=0),
     dict(M=16, iterations=20, step_size=3600.0, window=3600, initial_count=3, infect_prob=1.0,
          exposed_duration=3600, infectious_duration=3600, resistant_duration=100000000),
+    # long durations: more than 256 countdown values (16-bit codes on the batched path)
+    dict(M=40, iterations=140, step_size=1800.0, window=1800, initial_infected=0.05, infect_prob=0.2,
+         exposed_duration=100000, infectious_duration=200000, resistant_duration=100000000),
 ]
 
 
 @pytest.mark.parametrize("case", range(len(COUNTDOWN_CASES)))
-@pytest.mark.parametrize("csr", ["per-step", "prebuilt"])
-def test_countdown_replay_matches_oracle(rb, oracle, case, csr):
+@pytest.mark.parametrize("path,csr", [("plain", "per-step"), ("plain", "prebuilt"), ("batched", "per-step"),
+                                      ("batched", "prebuilt")])
+def test_countdown_replay_matches_oracle(rb, oracle, case, path, csr):
     from replay_b200 import synthetic
     net = synthetic.tiny(seed=10 + case, n_nodes=50, n_contacts=800)
     kw = dict(COUNTDOWN_CASES[case], start_time=net["t0"], seed=99 + case, transition="countdown")
     g = _graph(rb, net)
-    got = rb.Simulation(g, csr=csr, **kw).run()
+    got = rb.Simulation(g, path=path, csr=csr, **kw).run()
     want = oracle.run(net["start"], net["end"], net["u"], net["v"], net["n_nodes"], **_oracle_kw(kw))
     np.testing.assert_array_equal(got, want)
 
