@@ -43,6 +43,10 @@ def parse_args():
                          "hot: the sweep network with 5,000 initial infected for 12 steps; quiet: its "
                          "first 6 steps (profiler cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain-path / CPU / e2e legs")
+    ap.add_argument("--record-traffic", metavar="NCU_CSV",
+                    help="store the k_step DRAM bytes per launch of --workload from an ncu CSV in "
+                         "profiles/traffic.json and exit")
+    ap.add_argument("--capture", default="", help="the ncu command line that made --record-traffic's CSV")
     return ap.parse_args()
 
 
@@ -120,19 +124,54 @@ def workload(name):
     return net
 
 
+TRAFFIC_JSON = os.path.join(ROOT, "profiles", "traffic.json")
+
+
 def profiled_traffic(name):
-    """DRAM bytes per step (both step kernels) from the committed ncu summary of
-    this workload, or None: lines `traffic_bytes_per_step <workload> <bytes>`."""
-    path = os.path.join(ROOT, "profiles", "launches_replica_sweep.md")
+    """DRAM bytes per k_step launch of this workload, from profiles/traffic.json
+    (written by `bench.py --record-traffic` from an ncu capture), or None."""
     try:
-        with open(path) as f:
-            for line in f:
-                parts = line.strip().strip("`").split()
-                if len(parts) == 3 and parts[0] == "traffic_bytes_per_step" and parts[1] == name:
-                    return float(parts[2])
-    except OSError:
-        pass
-    return None
+        with open(TRAFFIC_JSON) as f:
+            d = json.load(f)
+    except (OSError, ValueError):
+        return None, None
+    w = d.get("workloads", {}).get(name)
+    if not w:
+        return None, None
+    return float(w["bytes_per_launch"]), w.get("capture")
+
+
+def record_traffic(csv_path, workload_name, capture):
+    """Reads an ncu CSV (`ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
+    ... --csv`) and stores the average DRAM bytes per k_step launch of the
+    workload in profiles/traffic.json."""
+    import csv
+    with open(csv_path) as f:
+        lines = [ln for ln in f if ln.startswith('"')]
+    per_launch = {}
+    for r in csv.DictReader(lines):
+        if "k_step" not in r.get("Kernel Name", ""):
+            continue
+        name, unit = r["Metric Name"], r.get("Metric Unit", "")
+        val = float(r["Metric Value"].replace(",", ""))
+        scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}.get(unit, 1)
+        if name in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            per_launch[r["ID"]] = per_launch.get(r["ID"], 0.0) + val * scale
+    rows = list(per_launch.values())
+    if not rows:
+        raise SystemExit(f"no k_step DRAM metrics in {csv_path}")
+    try:
+        with open(TRAFFIC_JSON) as f:
+            d = json.load(f)
+    except (OSError, ValueError):
+        d = {"kernel": "k_step", "metric": "dram__bytes_read.sum + dram__bytes_write.sum per launch",
+             "workloads": {}}
+    d["workloads"][workload_name] = {"bytes_per_launch": sum(rows) / len(rows), "launches": len(rows),
+                                     "min": min(rows), "max": max(rows), "capture": capture}
+    with open(TRAFFIC_JSON, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+        f.write("\n")
+    print(json.dumps(d["workloads"][workload_name]))
 
 
 def algorithmic_bytes(n, m, steps, nnz_total):
@@ -231,6 +270,10 @@ def run_ours(args, rank, world, local_rank):
                        "algorithmic_bytes_per_launch": bytes_replay / T,
                        "avg_launch_us": step_launch_ms * 1e3,
                        "traffic": None}
+    traffic, capture = profiled_traffic(args.workload)
+    if traffic is not None:
+        out["roofline"]["traffic"] = traffic
+        out["roofline"]["traffic_source"] = f"profiles/traffic.json: {capture}"
     out["profile_ms"] = {"per_step": prof} if args.no_extras else {"prebuilt": prof, "per_step": sim.profile()}
 
     if not args.no_extras and rank == 0:
@@ -251,17 +294,37 @@ def run_ours(args, rank, world, local_rank):
         # streams contact batches would keep them (staged once, untimed)
         host_in, pinned = pinned_inputs(net)
 
+        phases = {}
+
+        def lap(name, t0):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            phases[name] = phases.get(name, 0.0) + (t1 - t0) * 1e3
+            return t1
+
         def e2e_once():
+            t = time.perf_counter()
             ge = replay_b200.Graph.from_arrays(host_in["start"], host_in["end"], host_in["u"], host_in["v"],
                                                n_nodes, device=dev)
+            t = lap("graph_ms", t)
             se = replay_b200.Simulation(ge, path="batched", csr="per-step", **p)
+            t = lap("simulation_ms", t)
             c = se.run()
+            t = lap("run_ms", t)
+            gi, si = ge.info, se.info
+            for k in ("prep_ms", "build_ms"):
+                phases["graph." + k] = phases.get("graph." + k, 0.0) + gi[k]
+            for k in ("setup_ms", "alloc_ms", "prebuild_ms", "capture_ms"):
+                phases["simulation." + k] = phases.get("simulation." + k, 0.0) + si[k]
             se.close()
+            t = lap("close_simulation_ms", t)
             ge.close()
+            lap("close_graph_ms", t)
             return c
 
         for _ in range(e2e_warmup):
             e2e_once()
+        phases.clear()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
@@ -271,6 +334,7 @@ def run_ours(args, rank, world, local_rank):
         out["e2e"] = {"value": nrs_per_replay / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                       "d2h_bytes_per_step": d2h, "s_per_step": e2e_s,
                       "includes": "contact upload + interval index build + plan + replay + counts readback",
+                      "phases_ms": {k: v / e2e_steps for k, v in sorted(phases.items())},
                       "pinned_inputs": pinned, "warmup": e2e_warmup, "steps": e2e_steps}
         out["ingest_s"] = ingest_s
         assert counts.shape == (T + 1, M, 4)
@@ -284,7 +348,65 @@ def run_ours(args, rank, world, local_rank):
         out["uneven_batch"] = uneven_batch_leg(replay_b200, dev, timed)
         # ---- expected-value replay: forward, adjoint, beta calibration ----
         out["meanfield"] = meanfield_leg(replay_b200, g, net, p, nnz_total, hbm)
+        # ---- the reference arm's sample and rule, on our batched countdown path ----
+        out["reference_sample_countdown"] = reference_sample_leg(replay_b200, dev, timed, args)
+        # ---- dense stress: hub rows, 16,384 replicas ----
+        del sim_pre
+        out["dense_stress"] = dense_stress_leg(replay_b200, dev, timed, hbm)
     return out
+
+
+def reference_sample_leg(replay_b200, dev, timed, args):
+    """The reference arm's bounded sample (`bench.py --impl reference`: the
+    first 5,000 nodes' contacts, 64 replicas, all 336 steps, countdown rule
+    with durations equal to the geometric means) on our batched countdown
+    path: the same workload and rule as the reference's CPU number."""
+    net, sample, m = reference_sample(args.workload)
+    p = net["params"]
+    kw = reference_countdown_params(p, sample, m)
+    g = replay_b200.Graph.from_arrays(sample["start"], sample["end"], sample["u"], sample["v"],
+                                      sample["n_nodes"], device=dev)
+    sim = replay_b200.Simulation(g, path="batched", **kw)
+    ms = timed(sim, 3, 2) / 3
+    out = {"workload": f"reference arm's sample: {sample['n_nodes']} nodes, {len(sample['start'])} contacts, "
+                       f"{m} replicas, {p['iterations']} steps, countdown",
+           "ms_per_replay": ms, "value": sample["n_nodes"] * m * p["iterations"] / (ms / 1e3), "unit": UNIT,
+           "path": "batched countdown (replica codes)"}
+    sim.close()
+    g.close()
+    return out
+
+
+def dense_stress_leg(replay_b200, dev, timed, hbm):
+    """The dense stress configuration at full size (N = 5,000, 50M power-law
+    contacts, 2,880 x 15 min steps, 16,384 replicas, SIR): hub rows with
+    thousands of CSR entries per window.  One replay after a warm-up, window
+    CSRs built per step, with its own roofline over the step kernel."""
+    from replay_b200 import synthetic
+    net = synthetic.dense_stress()
+    p = dict(net["params"])
+    n, M, T = net["n_nodes"], p["M"], p["iterations"]
+    t0 = time.perf_counter()
+    g = replay_b200.Graph.from_arrays(net["start"], net["end"], net["u"], net["v"], n, device=dev)
+    ingest = time.perf_counter() - t0
+    sim = replay_b200.Simulation(g, path="batched", csr="per-step", **p)
+    ms = timed(sim, 1, 1)
+    prof = sim.profile()
+    sim.close()
+    pre = replay_b200.Simulation(g, path="batched", csr="prebuilt", **p)
+    nnz_total = pre.info["nnz_total"]
+    pre.close()
+    bytes_replay = algorithmic_bytes(n, M, T, nnz_total)
+    launch_ms = prof["step_ms"] / max(1, prof["step_launches"])
+    achieved = (bytes_replay / T) / (launch_ms / 1e3) / 1e9
+    g.close()
+    return {"workload": net["name"], "contacts": int(len(net["start"])), "ingest_s": ingest,
+            "ms_per_replay": ms, "value": n * M * T / (ms / 1e3), "unit": UNIT,
+            "nnz_per_step": nnz_total / T,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "kernel": "k_step", "algorithmic_bytes_per_launch": bytes_replay / T,
+                         "avg_launch_us": launch_ms * 1e3,
+                         "note": "the 10 MB infectious mask stays in L2: algorithmic gather bytes exceed DRAM traffic"}}
 
 
 def pinned_inputs(net):
@@ -508,6 +630,20 @@ def reference_sample(workload_name):
     return net, sample, m
 
 
+def reference_countdown_params(p, sample, m):
+    """The countdown rule of the reference arm's sample: infect-prob from the
+    sweep's median beta per contact-hour, durations equal to the geometric
+    means, resistance beyond the horizon, Bernoulli initial infection at the
+    workload's initial fraction."""
+    beta = float(np.median(p.get("beta_per_replica", [p.get("beta", 2e-5)])))
+    return dict(M=m, iterations=p["iterations"], step_size=p["step_size"], window=p["window"],
+                start_time=p["start_time"], transition="countdown",
+                initial_infected=p["initial_count"] / sample["n_nodes"],
+                infect_prob=float(1.0 - np.exp(-beta * 3600.0)),
+                exposed_duration=int(3600 / max(p.get("p_ei", 1 / 48), 1e-9)),
+                infectious_duration=int(3600 / p["p_ir"]), resistant_duration=10 ** 8)
+
+
 def run_reference(args):
     from oracle import ref
     from replay_b200 import synthetic
@@ -516,17 +652,17 @@ def run_reference(args):
     T = p["iterations"]
     if not os.path.exists(ref.REPLAY_REF):
         return {"impl": "reference", "unavailable": "oracle/_ref/replay_ref was not built (reference tree absent at build time)"}
-    beta = float(np.median(p.get("beta_per_replica", [p.get("beta", 2e-5)])))
-    infect_prob = 1.0 - np.exp(-beta * 3600.0)
+    kw = reference_countdown_params(p, sample, m)
     cores = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "contacts.txt")
         synthetic.write_contact_file(path, sample)
-        base = [path, "--cpu-only", "--cpu-threads", cores, "-q", "--M", m, "--step-size", p["step_size"],
-                "--static-network-duration", p["window"], "--start-time", p["start_time"],
-                "--initial-infected", p["initial_count"] / sample["n_nodes"], "--infect-prob", infect_prob,
-                "--exposed-duration", int(3600 / max(p.get("p_ei", 1 / 48), 1e-9)),
-                "--infectious-duration", int(3600 / p["p_ir"]), "--resistant-duration", 10 ** 8]
+        base = [path, "--cpu-only", "--cpu-threads", cores, "-q", "--M", m, "--step-size", kw["step_size"],
+                "--static-network-duration", kw["window"], "--start-time", kw["start_time"],
+                "--initial-infected", kw["initial_infected"], "--infect-prob", kw["infect_prob"],
+                "--exposed-duration", kw["exposed_duration"],
+                "--infectious-duration", kw["infectious_duration"],
+                "--resistant-duration", kw["resistant_duration"]]
         times = []
         for it in range(args.warmup + args.steps):
             t0 = time.perf_counter()
@@ -554,6 +690,9 @@ def run_reference(args):
 
 def main():
     args = parse_args()
+    if args.record_traffic:
+        record_traffic(args.record_traffic, args.workload, args.capture)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

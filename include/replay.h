@@ -61,6 +61,8 @@ typedef struct {
   int64_t t_max;       /* largest stored end */
   int32_t n_classes;   /* duration classes of the interval index */
   int32_t device;      /* CUDA device holding the index */
+  double prep_ms;      /* host time: argument checks, endpoint pass (from arrays) or parse (text) */
+  double build_ms;     /* host time of the upload and device index build (synchronised) */
 } rp_graph_info;
 
 /* Parses a contact file (NODE_LIST header, then `u, v, ISO8601, ISO8601;`
@@ -263,6 +265,11 @@ typedef struct {
   int64_t prebuilt_nnz;    /* total CSR entries when prebuilt */
   int64_t device_bytes;    /* device memory the handle holds */
   int64_t nnz_total;       /* sum over steps of CSR entries multiplied */
+  /* host time of rp_sim_create's phases, ms */
+  double setup_ms;         /* schedule, window plans, window workspaces */
+  double alloc_ms;         /* state, counters and count buffers */
+  double prebuild_ms;      /* every window CSR built once (prebuilt mode) */
+  double capture_ms;       /* CUDA graph capture and instantiation */
 } rp_sim_info;
 RP_API rp_status rp_sim_get_info(const rp_sim *s, rp_sim_info *out);
 

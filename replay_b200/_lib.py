@@ -23,7 +23,8 @@ CSR_MODE = {"per-step": 0, "prebuilt": 1}
 class GraphInfo(C.Structure):
     _fields_ = [("n_nodes", C.c_int32), ("n_index", C.c_int32), ("n_contacts", C.c_int64),
                 ("nlists", C.c_int64), ("n_malformed", C.c_int64), ("t_min", C.c_int64),
-                ("t_max", C.c_int64), ("n_classes", C.c_int32), ("device", C.c_int32)]
+                ("t_max", C.c_int64), ("n_classes", C.c_int32), ("device", C.c_int32),
+                ("prep_ms", C.c_double), ("build_ms", C.c_double)]
 
 
 class Params(C.Structure):
@@ -61,7 +62,9 @@ class Params(C.Structure):
 class SimInfo(C.Structure):
     _fields_ = [("path", C.c_int32), ("words", C.c_int32), ("n_windows", C.c_int32),
                 ("kernels_per_run", C.c_int32), ("max_candidates", C.c_int64),
-                ("prebuilt_nnz", C.c_int64), ("device_bytes", C.c_int64), ("nnz_total", C.c_int64)]
+                ("prebuilt_nnz", C.c_int64), ("device_bytes", C.c_int64), ("nnz_total", C.c_int64),
+                ("setup_ms", C.c_double), ("alloc_ms", C.c_double), ("prebuild_ms", C.c_double),
+                ("capture_ms", C.c_double)]
 
 
 class Profile(C.Structure):

@@ -7,6 +7,7 @@
 // is one graph launch.  No host synchronisation inside the step loop; only
 // the (n_steps+1) x M x 4 counts leave the device.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -176,6 +177,12 @@ int resolve_path(const rp_params &p) {
 
 using namespace rp;
 
+namespace {
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+}  // namespace
+
 struct rp_sim {
   const Graph *g = nullptr;
   rp_params p{};
@@ -230,6 +237,7 @@ struct rp_sim {
   cudaGraphExec_t exec = nullptr;
   int kernels_per_run = 0;
   int64_t nnz_total = 0;
+  double setup_ms = 0.0, alloc_ms = 0.0, prebuild_ms = 0.0, capture_ms = 0.0;
 
   ~rp_sim() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -795,6 +803,7 @@ RP_API rp_status rp_graph_load_text(const char *path, int device, rp_graph **out
   *out = nullptr;
   std::unique_ptr<rp_graph> h(new rp_graph());
   ParsedContacts pc;
+  const auto t0 = std::chrono::steady_clock::now();
   {
     // The device's context (a few hundred milliseconds to create, and
     // needing no input) is created on a helper thread while the file is
@@ -812,7 +821,11 @@ RP_API rp_status rp_graph_load_text(const char *path, int device, rp_graph **out
   h->g.device = device;
   h->g.n_index = pc.n_index;
   h->g.n_malformed = pc.n_malformed;
+  h->prep_ms = ms_since(t0);
+  const auto t1 = std::chrono::steady_clock::now();
   RP_TRY(graph_build_device(h->g, pc.start, pc.end, pc.u, pc.v, pc.n, pc.n_nodes));
+  RP_TRY_CUDA(cudaDeviceSynchronize());
+  h->build_ms = ms_since(t1);
   *out = h.release();
   return RP_OK;
 }
@@ -849,6 +862,7 @@ RP_API rp_status rp_graph_from_arrays(const int64_t *start, const int64_t *end,
     return RP_ERR_ARG;
   }
   *out = nullptr;
+  const auto t0 = std::chrono::steady_clock::now();
   std::vector<int32_t> uu(n_contacts), vv(n_contacts);
   std::vector<uint8_t> seen(n_nodes, 0);
   int32_t n_index = 0;
@@ -867,7 +881,11 @@ RP_API rp_status rp_graph_from_arrays(const int64_t *start, const int64_t *end,
   std::unique_ptr<rp_graph> h(new rp_graph());
   h->g.device = device;
   h->g.n_index = n_index;
+  h->prep_ms = ms_since(t0);
+  const auto t1 = std::chrono::steady_clock::now();
   RP_TRY(graph_build_device(h->g, start, end, uu.data(), vv.data(), n_contacts, n_nodes));
+  RP_TRY_CUDA(cudaDeviceSynchronize());
+  h->build_ms = ms_since(t1);
   *out = h.release();
   return RP_OK;
 }
@@ -887,6 +905,8 @@ RP_API rp_status rp_graph_get_info(const rp_graph *h, rp_graph_info *o) {
   o->t_max = g.t_max;
   o->n_classes = g.n_classes_used;
   o->device = g.device;
+  o->prep_ms = h->prep_ms;
+  o->build_ms = h->build_ms;
   return RP_OK;
 }
 
@@ -1016,11 +1036,17 @@ RP_API rp_status rp_sim_create_batch(const rp_graph *h, const rp_params *p,
     set_error("network offsets missing");
     return RP_ERR_ARG;
   }
+  auto t0 = std::chrono::steady_clock::now();
   RP_TRY(sim_setup(*s, h->g, *p));
+  s->setup_ms = ms_since(t0);
+  t0 = std::chrono::steady_clock::now();
   RP_TRY(alloc_state(*s));
+  s->alloc_ms = ms_since(t0);
   s->prebuilt = p->csr_mode == RP_CSR_PREBUILT;
+  t0 = std::chrono::steady_clock::now();
   if (s->prebuilt) {
     RP_TRY(prebuild(*s));
+    s->prebuild_ms = ms_since(t0);
   } else if (s->wins.size() > 1) {
     int64_t max_cand = 0;
     for (const WinDesc &d : s->wins) max_cand = std::max(max_cand, d.n_candidates);
@@ -1030,6 +1056,7 @@ RP_API rp_status rp_sim_create_batch(const rp_graph *h, const rp_params *p,
     for (cudaEvent_t *e : {&s->ev_built[0], &s->ev_built[1], &s->ev_free, &s->ev_join})
       RP_TRY_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     s->overlap = true;
+    s->setup_ms += ms_since(t0);
   }
   for (int32_t t = 0; t < s->T; ++t) {
     // nnz multiplied per step (for the roofline); per-step mode counts the
@@ -1041,7 +1068,9 @@ RP_API rp_status rp_sim_create_batch(const rp_graph *h, const rp_params *p,
       s->nnz_total += next - s->arena_ent_off[w];
     }
   }
+  t0 = std::chrono::steady_clock::now();
   if (!p->record_node_states) RP_TRY(capture(*s));
+  s->capture_ms = ms_since(t0);
   *out = s.release();
   return RP_OK;
 }
@@ -1172,6 +1201,10 @@ RP_API rp_status rp_sim_get_info(const rp_sim *s, rp_sim_info *o) {
   for (auto b : bufs) bytes += (int64_t)b->bytes;
   o->device_bytes = bytes;
   o->nnz_total = s->nnz_total;
+  o->setup_ms = s->setup_ms;
+  o->alloc_ms = s->alloc_ms;
+  o->prebuild_ms = s->prebuild_ms;
+  o->capture_ms = s->capture_ms;
   return RP_OK;
 }
 

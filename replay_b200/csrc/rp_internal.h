@@ -310,4 +310,5 @@ void plain_spmv_f32_raw(const int32_t *row_ptr, const int32_t *col,
 
 struct rp_graph {
   rp::Graph g;
+  double prep_ms = 0.0, build_ms = 0.0;  // creation phases (rp_graph_info)
 };
