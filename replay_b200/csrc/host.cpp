@@ -477,7 +477,21 @@ struct rp_meanfield {
   DevBuf inc_part;             // T x blocks incidence partials
   DevBuf a0, a1, z0, z1;       // adjoint ping-pong (4N), coupling terms (N)
   DevBuf gpart;                // blocks x 4 FP64 scalar-gradient partials
-  DevBuf sus;                  // copy of the forward's susceptibility
+  DevBuf sus;                  // copy of the forward's susceptibility (ones when none)
+  DevBuf ones;                 // N x 1.0f
+  DevBuf d_rates;              // MfRates read by the kernels
+  DevBuf inc, ginc;            // T incidences; T incidence gradients
+  DevBuf gx0, gsus, grates;    // adjoint outputs
+  // the whole forward and the whole adjoint, captured once on `cap` (all
+  // pointers internal) and replayed on the caller's stream
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t fwd = nullptr, bwd = nullptr;
+  const float *final_x = nullptr;  // x_T inside the forward's buffers
+  ~rp_meanfield() {
+    if (fwd) cudaGraphExecDestroy(fwd);
+    if (bwd) cudaGraphExecDestroy(bwd);
+    if (cap) cudaStreamDestroy(cap);
+  }
 };
 
 namespace {
@@ -772,6 +786,98 @@ rp_status capture(rp_sim &s) {
 }
 
 }  // namespace
+
+// Captures stream work enqueued by `body` on m.cap into an executable graph.
+template <typename F>
+rp_status mf_capture(rp_meanfield &m, cudaGraphExec_t &exec, F body) {
+  cudaGraph_t graph = nullptr;
+  RP_TRY_CUDA(cudaStreamBeginCapture(m.cap, cudaStreamCaptureModeThreadLocal));
+  rp_status st = body(m.cap);
+  cudaError_t e = cudaStreamEndCapture(m.cap, &graph);
+  if (st != RP_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (mean-field)");
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate (mean-field)");
+  return RP_OK;
+}
+
+// The forward over every step from ckpt[0]: states ping-pong in xa/xb,
+// checkpoints every K steps, per-step incidence into m.inc.
+rp_status mf_capture_forward(rp_meanfield &m) {
+  const int32_t N = m.N, T = m.T;
+  const size_t plane = sizeof(float) * 4 * (size_t)N;
+  float *ck = m.ckpt.as<float>();
+  float *pp[2] = {m.xa.as<float>(), m.xb.as<float>()};
+  m.final_x = T > 0 ? pp[(T - 1) & 1] : ck;
+  return mf_capture(m, m.fwd, [&](cudaStream_t st) -> rp_status {
+    const float *x = ck;
+    for (int32_t t = 0; t < T; ++t) {
+      float *nxt = pp[t & 1];
+      mf_step(m.base.rp_of(t), m.base.ent_of(t), N, m.base.step_scale[t],
+              m.d_rates.as<MfRates>(), m.sus.as<float>(), x, nxt, nullptr, nullptr,
+              m.inc_part.as<float>() + (size_t)t * m.nblk, st);
+      if ((t + 1) % m.K == 0 && t + 1 < T)
+        RP_TRY_CUDA(cudaMemcpyAsync(ck + (size_t)((t + 1) / m.K) * 4 * N, nxt, plane,
+                                    cudaMemcpyDeviceToDevice, st));
+      x = nxt;
+    }
+    mf_incidence(m.inc_part.as<float>(), m.nblk, T, m.inc.as<float>(), st);
+    return RP_OK;
+  });
+}
+
+// The adjoint from y = a0 (dL/dx_T) and m.ginc (dL/dincidence) back to
+// dL/dx_0 (gx0), with dL/ds (gsus) and the FP64 rate gradients (grates):
+// per checkpoint segment the states, exp(-beta s e) and scaled exposures
+// are recomputed, then one kernel per reverse step.
+rp_status mf_capture_backward(rp_meanfield &m) {
+  const int32_t N = m.N, T = m.T, K = m.K;
+  const size_t plane = sizeof(float) * 4 * (size_t)N;
+  return mf_capture(m, m.bwd, [&](cudaStream_t st) -> rp_status {
+    const float *sus = m.sus.as<float>();
+    const MfRates *r = m.d_rates.as<MfRates>();
+    RP_TRY_CUDA(cudaMemsetAsync(m.gpart.ptr, 0, m.gpart.bytes, st));
+    RP_TRY_CUDA(cudaMemsetAsync(m.gsus.ptr, 0, sizeof(float) * (size_t)N, st));
+    float *a[2] = {m.a0.as<float>(), m.a1.as<float>()};
+    float *z[2] = {m.z0.as<float>(), m.z1.as<float>()};
+    int ai = 0;
+    const float *ck = m.ckpt.as<float>();
+    float *sx = m.seg_x.as<float>(), *sq = m.seg_q.as<float>(), *se = m.seg_e.as<float>();
+    // x of step t within the recomputed segment starting at c0
+    auto seg_state = [&](int32_t c0, int32_t t) -> const float * {
+      return t == c0 ? ck + (size_t)(c0 / K) * 4 * N : sx + (size_t)(t - c0) * 4 * N;
+    };
+    for (int32_t t = T - 1; t >= 0; --t) {
+      const int32_t c0 = (t / K) * K;
+      if (t == T - 1 || t == c0 + K - 1) {
+        for (int32_t u = c0; u <= t; ++u) {
+          float *xo = u + 1 <= t ? sx + (size_t)(u + 1 - c0) * 4 * N : m.xa.as<float>();
+          mf_step(m.base.rp_of(u), m.base.ent_of(u), N, m.base.step_scale[u], r, sus,
+                  seg_state(c0, u), xo, sq + (size_t)(u - c0) * N, se + (size_t)(u - c0) * N,
+                  m.inc_part.as<float>() + (size_t)u * m.nblk, st);
+        }
+      }
+      const bool couple = t + 1 < T;
+      mf_adjoint(N, couple ? m.base.rp_of(t + 1) : nullptr,
+                 couple ? m.base.ent_of(t + 1) : nullptr, z[(t + 1) & 1], a[ai],
+                 seg_state(c0, t), sq + (size_t)(t - c0) * N, se + (size_t)(t - c0) * N,
+                 m.ginc.as<float>(), t, m.base.step_scale[t], r, sus, a[ai ^ 1], z[t & 1],
+                 m.gsus.as<float>(), m.gpart.as<double>(), st);
+      ai ^= 1;
+    }
+    if (T > 0)
+      mf_adjoint(N, m.base.rp_of(0), m.base.ent_of(0), z[0], a[ai], nullptr, nullptr, nullptr,
+                 nullptr, 0, 1.0f, r, sus, m.gx0.as<float>(), nullptr, nullptr, nullptr, st);
+    else
+      RP_TRY_CUDA(cudaMemcpyAsync(m.gx0.ptr, a[ai], plane, cudaMemcpyDeviceToDevice, st));
+    mf_finish(m.gpart.as<double>(), m.nblk, m.grates.as<double>(), st);
+    return RP_OK;
+  });
+}
 
 // Fails when a kernel of the last replay gave up a bounded wait (the flag is
 // sticky until read here).
@@ -1440,6 +1546,19 @@ RP_API rp_status rp_meanfield_create(const rp_graph *h, const rp_params *p,
   RP_TRY(m->z1.alloc(sizeof(float) * (size_t)N));
   RP_TRY(m->gpart.alloc(sizeof(double) * 4 * (size_t)m->nblk));
   RP_TRY(m->sus.alloc(sizeof(float) * (size_t)N));
+  RP_TRY(m->ones.alloc(sizeof(float) * (size_t)N));
+  {
+    std::vector<float> one((size_t)N, 1.0f);
+    RP_TRY_CUDA(cudaMemcpy(m->ones.ptr, one.data(), sizeof(float) * (size_t)N,
+                           cudaMemcpyHostToDevice));
+  }
+  RP_TRY(m->d_rates.alloc(sizeof(MfRates)));
+  RP_TRY(m->inc.alloc(sizeof(float) * (size_t)(T > 0 ? T : 1)));
+  RP_TRY(m->ginc.alloc(sizeof(float) * (size_t)(T > 0 ? T : 1)));
+  RP_TRY(m->gx0.alloc(plane));
+  RP_TRY(m->gsus.alloc(sizeof(float) * (size_t)N));
+  RP_TRY(m->grates.alloc(sizeof(double) * 4));
+  RP_TRY_CUDA(cudaStreamCreateWithFlags(&m->cap, cudaStreamNonBlocking));
   m->rates.has_exposed = p->has_exposed;
   m->rates.ir_to_s = p->ir_to_s;
   *out = m.release();
@@ -1469,25 +1588,19 @@ RP_API rp_status rp_meanfield_forward(rp_meanfield *m, const float *d_x0, float 
   m->rates.p_ir = p_ir;
   m->rates.p_rs = p_rs;
   m->has_sus = d_sus != nullptr;
-  if (d_sus)
-    RP_TRY_CUDA(cudaMemcpyAsync(m->sus.ptr, d_sus, sizeof(float) * (size_t)N,
+  if (!m->fwd) RP_TRY(mf_capture_forward(*m));
+  // inputs into the graph's fixed buffers (a missing susceptibility is a
+  // vector of ones: the products it enters are then exact)
+  RP_TRY_CUDA(cudaMemcpyAsync(m->d_rates.ptr, &m->rates, sizeof(MfRates), cudaMemcpyHostToDevice,
+                              st));
+  RP_TRY_CUDA(cudaMemcpyAsync(m->sus.ptr, d_sus ? d_sus : m->ones.as<float>(),
+                              sizeof(float) * (size_t)N, cudaMemcpyDeviceToDevice, st));
+  RP_TRY_CUDA(cudaMemcpyAsync(m->ckpt.ptr, d_x0, plane, cudaMemcpyDeviceToDevice, st));
+  RP_TRY_CUDA(cudaGraphLaunch(m->fwd, st));
+  if (d_incidence && T > 0)
+    RP_TRY_CUDA(cudaMemcpyAsync(d_incidence, m->inc.ptr, sizeof(float) * (size_t)T,
                                 cudaMemcpyDeviceToDevice, st));
-  const float *sus = m->has_sus ? m->sus.as<float>() : nullptr;
-  float *ck = m->ckpt.as<float>();
-  RP_TRY_CUDA(cudaMemcpyAsync(ck, d_x0, plane, cudaMemcpyDeviceToDevice, st));
-  const float *cur = ck;
-  float *pp[2] = {m->xa.as<float>(), m->xb.as<float>()};
-  for (int32_t t = 0; t < T; ++t) {
-    float *nxt = pp[t & 1];
-    mf_step(m->base.rp_of(t), m->base.ent_of(t), N, m->base.step_scale[t], m->rates, sus, cur,
-            nxt, nullptr, nullptr, m->inc_part.as<float>() + (size_t)t * m->nblk, st);
-    if ((t + 1) % m->K == 0 && t + 1 < T)
-      RP_TRY_CUDA(cudaMemcpyAsync(ck + (size_t)((t + 1) / m->K) * 4 * N, nxt, plane,
-                                  cudaMemcpyDeviceToDevice, st));
-    cur = nxt;
-  }
-  if (d_incidence) mf_incidence(m->inc_part.as<float>(), m->nblk, T, d_incidence, st);
-  if (d_xT) RP_TRY_CUDA(cudaMemcpyAsync(d_xT, cur, plane, cudaMemcpyDeviceToDevice, st));
+  if (d_xT) RP_TRY_CUDA(cudaMemcpyAsync(d_xT, m->final_x, plane, cudaMemcpyDeviceToDevice, st));
   RP_TRY_CUDA(cudaGetLastError());
   m->have_forward = true;
   return RP_OK;
@@ -1506,50 +1619,29 @@ RP_API rp_status rp_meanfield_backward(rp_meanfield *m, const float *d_grad_inci
   }
   RP_TRY_CUDA(cudaSetDevice(m->base.g->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int32_t N = m->N, T = m->T, K = m->K;
+  const int32_t N = m->N, T = m->T;
   const size_t plane = sizeof(float) * 4 * (size_t)N;
-  const float *sus = m->has_sus ? m->sus.as<float>() : nullptr;
-  const MfRates &r = m->rates;
-  RP_TRY_CUDA(cudaMemsetAsync(m->gpart.ptr, 0, m->gpart.bytes, st));
-  if (d_grad_sus) RP_TRY_CUDA(cudaMemsetAsync(d_grad_sus, 0, sizeof(float) * (size_t)N, st));
-  float *a[2] = {m->a0.as<float>(), m->a1.as<float>()};
-  float *z[2] = {m->z0.as<float>(), m->z1.as<float>()};
+  if (!m->bwd) RP_TRY(mf_capture_backward(*m));
+  // inputs into the graph's fixed buffers: a missing gradient is zero
   if (d_grad_xT)
-    RP_TRY_CUDA(cudaMemcpyAsync(a[0], d_grad_xT, plane, cudaMemcpyDeviceToDevice, st));
+    RP_TRY_CUDA(cudaMemcpyAsync(m->a0.ptr, d_grad_xT, plane, cudaMemcpyDeviceToDevice, st));
   else
-    RP_TRY_CUDA(cudaMemsetAsync(a[0], 0, plane, st));
-  int ai = 0;
-  const float *ck = m->ckpt.as<float>();
-  float *sx = m->seg_x.as<float>(), *sq = m->seg_q.as<float>(), *se = m->seg_e.as<float>();
-  // x of step t within the recomputed segment starting at c0
-  auto seg_state = [&](int32_t c0, int32_t t) -> const float * {
-    return t == c0 ? ck + (size_t)(c0 / K) * 4 * N : sx + (size_t)(t - c0) * 4 * N;
-  };
-  for (int32_t t = T - 1; t >= 0; --t) {
-    const int32_t c0 = (t / K) * K;
-    if (t == T - 1 || t == c0 + K - 1) {
-      // recompute the segment [c0, t]: states, exp(-beta s e) and scaled exposures
-      for (int32_t u = c0; u <= t; ++u) {
-        float *xo = u + 1 <= t ? sx + (size_t)(u + 1 - c0) * 4 * N : m->xa.as<float>();
-        mf_step(m->base.rp_of(u), m->base.ent_of(u), N, m->base.step_scale[u], r, sus,
-                seg_state(c0, u), xo, sq + (size_t)(u - c0) * N, se + (size_t)(u - c0) * N,
-                m->inc_part.as<float>() + (size_t)u * m->nblk, st);
-      }
-    }
-    const bool couple = t + 1 < T;
-    mf_adjoint(N, couple ? m->base.rp_of(t + 1) : nullptr,
-               couple ? m->base.ent_of(t + 1) : nullptr, z[(t + 1) & 1], a[ai],
-               seg_state(c0, t), sq + (size_t)(t - c0) * N, se + (size_t)(t - c0) * N,
-               d_grad_incidence, t, m->base.step_scale[t], r, sus, a[ai ^ 1], z[t & 1],
-               d_grad_sus, m->gpart.as<double>(), st);
-    ai ^= 1;
+    RP_TRY_CUDA(cudaMemsetAsync(m->a0.ptr, 0, plane, st));
+  if (T > 0) {
+    if (d_grad_incidence)
+      RP_TRY_CUDA(cudaMemcpyAsync(m->ginc.ptr, d_grad_incidence, sizeof(float) * (size_t)T,
+                                  cudaMemcpyDeviceToDevice, st));
+    else
+      RP_TRY_CUDA(cudaMemsetAsync(m->ginc.ptr, 0, sizeof(float) * (size_t)T, st));
   }
-  if (T > 0)
-    mf_adjoint(N, m->base.rp_of(0), m->base.ent_of(0), z[0], a[ai], nullptr, nullptr, nullptr,
-               nullptr, 0, 1.0f, r, sus, d_grad_x0, nullptr, nullptr, nullptr, st);
-  else
-    RP_TRY_CUDA(cudaMemcpyAsync(d_grad_x0, a[ai], plane, cudaMemcpyDeviceToDevice, st));
-  if (d_grad_rates) mf_finish(m->gpart.as<double>(), m->nblk, d_grad_rates, st);
+  RP_TRY_CUDA(cudaGraphLaunch(m->bwd, st));
+  RP_TRY_CUDA(cudaMemcpyAsync(d_grad_x0, m->gx0.ptr, plane, cudaMemcpyDeviceToDevice, st));
+  if (d_grad_sus)
+    RP_TRY_CUDA(cudaMemcpyAsync(d_grad_sus, m->gsus.ptr, sizeof(float) * (size_t)N,
+                                cudaMemcpyDeviceToDevice, st));
+  if (d_grad_rates)
+    RP_TRY_CUDA(cudaMemcpyAsync(d_grad_rates, m->grates.ptr, sizeof(double) * 4,
+                                cudaMemcpyDeviceToDevice, st));
   RP_TRY_CUDA(cudaGetLastError());
   return RP_OK;
 }

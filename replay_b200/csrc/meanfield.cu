@@ -27,6 +27,9 @@
 // One kernel per reverse step finishes dL/dx_t of a row (gather of z_t over
 // its neighbours) and immediately takes the local part of step t-1 for the
 // same row.  Scalar gradients accumulate in FP64, per block, in fixed order.
+// The kernels read the rates from device memory, so that the host captures
+// a whole forward (and a whole adjoint) once as a CUDA graph and replays it
+// for any beta and rates.
 #include "rp_device.cuh"
 #include "rp_internal.h"
 
@@ -66,10 +69,11 @@ __device__ __forceinline__ float row_exposure(const int32_t *__restrict__ rp,
 
 __global__ void __launch_bounds__(kMfThreads)
     k_mf_step(const int32_t *__restrict__ rp, const int2 *__restrict__ ent, int32_t n, float scale,
-              MfRates r, const float *__restrict__ sus, const float *__restrict__ x,
+              const MfRates *__restrict__ rates, const float *__restrict__ sus, const float *__restrict__ x,
               float *__restrict__ xo, float *__restrict__ q_out, float *__restrict__ e_out,
               float *__restrict__ inc_part) {
   __shared__ float sh[32];
+  const MfRates r = *rates;
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   float newinf = 0.0f;
   if (i < n) {
@@ -115,11 +119,12 @@ __global__ void __launch_bounds__(kMfThreads)
                  const float *__restrict__ z_in, const float *__restrict__ a_in,
                  const float *__restrict__ x, const float *__restrict__ qv,
                  const float *__restrict__ ev, const float *__restrict__ ginc, int32_t tl,
-                 float scale, MfRates r,
+                 float scale, const MfRates *__restrict__ rates,
                  const float *__restrict__ sus,
                  float *__restrict__ a_out, float *__restrict__ z_out, float *__restrict__ gsus,
                  double *__restrict__ gpart) {
   __shared__ double sh[32];
+  const MfRates r = *rates;
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   double gb = 0.0, ge = 0.0, gi = 0.0, gr = 0.0;
   if (i < n) {
@@ -180,7 +185,7 @@ __global__ void k_mf_finish(const double *__restrict__ gpart, int32_t nblk,
 
 int32_t mf_blocks(int32_t n) { return (n + kMfThreads - 1) / kMfThreads; }
 
-void mf_step(const int32_t *rp, const int2 *ent, int32_t n, float scale, const MfRates &r,
+void mf_step(const int32_t *rp, const int2 *ent, int32_t n, float scale, const MfRates *r,
              const float *sus, const float *x, float *xo, float *q_out, float *e_out,
              float *inc_part, cudaStream_t st) {
   k_mf_step<<<mf_blocks(n), kMfThreads, 0, st>>>(rp, ent, n, scale, r, sus, x, xo, q_out, e_out,
@@ -194,7 +199,7 @@ void mf_incidence(const float *part, int32_t nblk, int32_t T, float *inc, cudaSt
 
 void mf_adjoint(int32_t n, const int32_t *rp_c, const int2 *ent_c, const float *z_in,
                 const float *a_in, const float *x, const float *q, const float *e,
-                const float *ginc, int32_t tl, float scale, const MfRates &r, const float *sus,
+                const float *ginc, int32_t tl, float scale, const MfRates *r, const float *sus,
                 float *a_out, float *z_out, float *gsus, double *gpart, cudaStream_t st) {
   k_mf_adjoint<<<mf_blocks(n), kMfThreads, 0, st>>>(n, rp_c, ent_c, z_in, a_in, x, q, e, ginc, tl,
                                                    scale, r, sus, a_out, z_out, gsus, gpart);

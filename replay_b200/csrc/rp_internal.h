@@ -178,13 +178,13 @@ struct MfRates {
   int32_t has_exposed, ir_to_s;
 };
 int32_t mf_blocks(int32_t n);
-void mf_step(const int32_t *rp, const int2 *ent, int32_t n, float scale, const MfRates &r,
+void mf_step(const int32_t *rp, const int2 *ent, int32_t n, float scale, const MfRates *r,
              const float *sus, const float *x, float *xo, float *q_out, float *e_out,
              float *inc_part, cudaStream_t st);
 void mf_incidence(const float *part, int32_t nblk, int32_t T, float *inc, cudaStream_t st);
 void mf_adjoint(int32_t n, const int32_t *rp_c, const int2 *ent_c, const float *z_in,
                 const float *a_in, const float *x, const float *q, const float *e,
-                const float *ginc, int32_t tl, float scale, const MfRates &r, const float *sus,
+                const float *ginc, int32_t tl, float scale, const MfRates *r, const float *sus,
                 float *a_out, float *z_out, float *gsus, double *gpart, cudaStream_t st);
 void mf_finish(const double *gpart, int32_t nblk, double *out, cudaStream_t st);
 

@@ -7,9 +7,12 @@ the forward kernels on the current torch stream and returns
     incidence  (iterations,)  expected new infections per step
     x_T        (4, N)         final S, E, I, R probabilities
 
-as tensors of a torch.autograd.Function whose backward is the hand-written
-reverse-time adjoint (rp_meanfield_backward): gradients flow to x0, beta,
-the per-node susceptibility and the E->I, I->R, R->S rates.
+through the op `torch.ops.replay_b200.meanfield`, registered with the torch
+dispatcher (torch.library.custom_op, with a fake implementation for shape
+propagation) and with the hand-written reverse-time adjoint
+(rp_meanfield_backward) as its autograd formula: gradients flow to x0, beta,
+the per-node susceptibility and the E->I, I->R, R->S rates.  The library
+replays the whole forward (and adjoint) as one captured CUDA graph.
 
     mf = MeanField(g, iterations=336, step_size=3600, window=3600, start_time=t0)
     inc, xT = mf(x0, beta, susceptibility=s, p_ei=1/48, p_ir=1/120)
@@ -20,13 +23,14 @@ Everything runs on the GPU through libreplay; there is no CPU path.
 """
 import ctypes as C
 import math
+from typing import Optional, Tuple
 
 import torch
 
 from . import _lib
 from ._lib import check, lib
 
-__all__ = ["MeanField", "daily_incidence", "calibrate_beta"]
+__all__ = ["MeanField", "meanfield_op", "daily_incidence", "calibrate_beta"]
 
 
 def _scalar(v, like):
@@ -35,36 +39,59 @@ def _scalar(v, like):
     return torch.tensor(float(v), dtype=torch.float32, device=like.device)
 
 
-class _MeanFieldFn(torch.autograd.Function):
-    @staticmethod
-    def forward(ctx, mf, x0, beta, sus, p_ei, p_ir, p_rs):
-        x0c = x0.detach().to(torch.float32).contiguous()
-        susc = sus.detach().to(torch.float32).contiguous() if sus is not None else None
-        rates = [float(v) for v in (beta, p_ei, p_ir, p_rs)]
-        inc, xT = mf._forward(x0c, susc, rates)
-        ctx.mf = mf
-        ctx.generation = mf._generation
-        ctx.inputs = (x0c, susc, rates)
-        ctx.has_sus = sus is not None
-        ctx.rate_dtypes = [getattr(v, "dtype", torch.float32) for v in (beta, p_ei, p_ir, p_rs)]
-        return inc, xT
+# Live MeanField objects by handle id: the registered op takes the id (an
+# int) in place of the Python object.
+_LIVE = {}
 
-    @staticmethod
-    def backward(ctx, g_inc, g_xT):
-        mf = ctx.mf
-        if mf._generation != ctx.generation:  # another forward ran since: restore its checkpoints
-            mf._forward(*ctx.inputs)
-        dev = mf.device
-        g_inc = g_inc.to(torch.float32).contiguous() if g_inc is not None else None
-        g_xT = g_xT.to(torch.float32).contiguous() if g_xT is not None else None
-        gx0 = torch.empty((4, mf.N), dtype=torch.float32, device=dev)
-        gsus = torch.empty(mf.N, dtype=torch.float32, device=dev) if ctx.has_sus else None
-        grates = torch.empty(4, dtype=torch.float64, device=dev)
-        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
-        check(lib().rp_meanfield_backward(mf._h, ptr(g_inc), ptr(g_xT), ptr(gx0), ptr(gsus), ptr(grates),
-                                          C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
-        g = [grates[k].to(ctx.rate_dtypes[k]) for k in range(4)]
-        return None, gx0, g[0], gsus, g[1], g[2], g[3]
+
+@torch.library.custom_op("replay_b200::meanfield", mutates_args=())
+def meanfield_op(handle: int, x0: torch.Tensor, beta: torch.Tensor, sus: Optional[torch.Tensor],
+                 p_ei: torch.Tensor, p_ir: torch.Tensor, p_rs: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Expected-value replay of MeanField `handle` (rp_meanfield_forward):
+    returns (incidence (T,), x_T (4, N)) in float32 on the graph's GPU."""
+    mf = _LIVE[handle]
+    x0c = x0.detach().to(torch.float32).contiguous()
+    susc = sus.detach().to(torch.float32).contiguous() if sus is not None else None
+    return mf._forward(x0c, susc, [float(v) for v in (beta, p_ei, p_ir, p_rs)])
+
+
+@meanfield_op.register_fake
+def _(handle, x0, beta, sus, p_ei, p_ir, p_rs):
+    mf = _LIVE[handle]
+    return x0.new_empty((mf.T,), dtype=torch.float32), x0.new_empty((4, mf.N), dtype=torch.float32)
+
+
+def _setup_context(ctx, inputs, output):
+    handle, x0, beta, sus, p_ei, p_ir, p_rs = inputs
+    mf = _LIVE[handle]
+    ctx.handle = handle
+    ctx.generation = mf._generation
+    ctx.inputs = (x0.detach().to(torch.float32).contiguous(),
+                  sus.detach().to(torch.float32).contiguous() if sus is not None else None,
+                  [float(v) for v in (beta, p_ei, p_ir, p_rs)])
+    ctx.has_sus = sus is not None
+    ctx.rate_dtypes = [v.dtype for v in (beta, p_ei, p_ir, p_rs)]
+
+
+def _backward(ctx, g_inc, g_xT):
+    """The reverse-time adjoint (rp_meanfield_backward)."""
+    mf = _LIVE[ctx.handle]
+    if mf._generation != ctx.generation:  # another forward ran since: restore its checkpoints
+        mf._forward(*ctx.inputs)
+    dev = mf.device
+    g_inc = g_inc.to(torch.float32).contiguous() if g_inc is not None else None
+    g_xT = g_xT.to(torch.float32).contiguous() if g_xT is not None else None
+    gx0 = torch.empty((4, mf.N), dtype=torch.float32, device=dev)
+    gsus = torch.empty(mf.N, dtype=torch.float32, device=dev) if ctx.has_sus else None
+    grates = torch.empty(4, dtype=torch.float64, device=dev)
+    ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+    check(lib().rp_meanfield_backward(mf._h, ptr(g_inc), ptr(g_xT), ptr(gx0), ptr(gsus), ptr(grates),
+                                      C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+    g = [grates[k].to(ctx.rate_dtypes[k]) for k in range(4)]
+    return None, gx0, g[0], gsus, g[1], g[2], g[3]
+
+
+meanfield_op.register_autograd(_backward, setup_context=_setup_context)
 
 
 class MeanField:
@@ -95,6 +122,8 @@ class MeanField:
         check(lib().rp_meanfield_create(graph._h, C.byref(p), int(checkpoint_every), C.byref(h)))
         self._h = h
         self._generation = 0
+        self.handle = h.value
+        _LIVE[self.handle] = self
 
     def _forward(self, x0, sus, rates):
         if x0.shape != (4, self.N) or x0.device != self.device:
@@ -115,10 +144,11 @@ class MeanField:
         x0 = x0.reshape(4, self.N)
         beta = _scalar(beta, x0)
         p_ei, p_ir, p_rs = (_scalar(v, x0) for v in (p_ei, p_ir, p_rs))
-        return _MeanFieldFn.apply(self, x0, beta, susceptibility, p_ei, p_ir, p_rs)
+        return torch.ops.replay_b200.meanfield(self.handle, x0, beta, susceptibility, p_ei, p_ir, p_rs)
 
     def close(self):
         if self._h and self._h.value:
+            _LIVE.pop(self.handle, None)
             lib().rp_meanfield_free(self._h)
             self._h = C.c_void_p()
 
