@@ -44,7 +44,7 @@ def parse_args():
                          "first 6 steps (profiler cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain-path / CPU / e2e legs")
     ap.add_argument("--record-traffic", metavar="NCU_CSV",
-                    help="store the k_step DRAM bytes per launch of --workload from an ncu CSV in "
+                    help="store the step kernels' DRAM bytes per step of --workload from an ncu CSV in "
                          "profiles/traffic.json and exit")
     ap.add_argument("--capture", default="", help="the ncu command line that made --record-traffic's CSV")
     return ap.parse_args()
@@ -128,7 +128,7 @@ TRAFFIC_JSON = os.path.join(ROOT, "profiles", "traffic.json")
 
 
 def profiled_traffic(name):
-    """DRAM bytes per k_step launch of this workload, from profiles/traffic.json
+    """DRAM bytes per step (k_infect + k_flow) of this workload, from profiles/traffic.json
     (written by `bench.py --record-traffic` from an ncu capture), or None."""
     try:
         with open(TRAFFIC_JSON) as f:
@@ -143,30 +143,36 @@ def profiled_traffic(name):
 
 def record_traffic(csv_path, workload_name, capture):
     """Reads an ncu CSV (`ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
-    ... --csv`) and stores the average DRAM bytes per k_step launch of the
-    workload in profiles/traffic.json."""
+    ... --csv`) and stores the DRAM bytes per step (k_infect + k_flow, one
+    launch each, averaged over the captured steps) of the workload in
+    profiles/traffic.json."""
     import csv
     with open(csv_path) as f:
         lines = [ln for ln in f if ln.startswith('"')]
     per_launch = {}
     for r in csv.DictReader(lines):
-        if "k_step" not in r.get("Kernel Name", ""):
+        kname = r.get("Kernel Name", "")
+        if "k_infect" not in kname and "k_flow" not in kname:
             continue
         name, unit = r["Metric Name"], r.get("Metric Unit", "")
         val = float(r["Metric Value"].replace(",", ""))
         scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}.get(unit, 1)
         if name in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
-            per_launch[r["ID"]] = per_launch.get(r["ID"], 0.0) + val * scale
-    rows = list(per_launch.values())
-    if not rows:
-        raise SystemExit(f"no k_step DRAM metrics in {csv_path}")
+            k = "k_infect" if "k_infect" in kname else "k_flow"
+            per_launch.setdefault(k, {})[r["ID"]] = per_launch.get(k, {}).get(r["ID"], 0.0) + val * scale
+    if not per_launch.get("k_infect") or not per_launch.get("k_flow"):
+        raise SystemExit(f"no k_infect / k_flow DRAM metrics in {csv_path}")
+    inf, flo = list(per_launch["k_infect"].values()), list(per_launch["k_flow"].values())
+    rows = [a + b for a, b in zip(inf, flo)]
     try:
         with open(TRAFFIC_JSON) as f:
             d = json.load(f)
     except (OSError, ValueError):
-        d = {"kernel": "k_step", "metric": "dram__bytes_read.sum + dram__bytes_write.sum per launch",
+        d = {"kernel": "k_infect + k_flow",
+             "metric": "dram__bytes_read.sum + dram__bytes_write.sum of the two launches of a step",
              "workloads": {}}
-    d["workloads"][workload_name] = {"bytes_per_launch": sum(rows) / len(rows), "launches": len(rows),
+    d["workloads"][workload_name] = {"bytes_per_launch": sum(rows) / len(rows), "steps": len(rows),
+                                     "k_infect": sum(inf) / len(inf), "k_flow": sum(flo) / len(flo),
                                      "min": min(rows), "max": max(rows), "capture": capture}
     with open(TRAFFIC_JSON, "w") as f:
         json.dump(d, f, indent=1, sort_keys=True)
@@ -258,17 +264,20 @@ def run_ours(args, rank, world, local_rank):
         out["prebuilt_csr"] = {"value": nrs_per_replay * world / (ms_pre / 1e3), "ms_per_step": ms_pre,
                                "prebuilt_nnz": sim_pre.info["prebuilt_nnz"]}
 
-    # ---- roofline of the step: k_step, one launch per step ----
+    # ---- roofline of the step: k_infect + k_flow, one launch each per step ----
     hbm, peak_kind = load_peaks()
     prof = prof_ps if args.no_extras else sim_pre.profile()
     bytes_replay = algorithmic_bytes(n_nodes, M, T, nnz_total)
-    step_launch_ms = prof["step_ms"] / max(1, prof["step_launches"])
+    infect_ms = prof["spmv_ms"] / max(1, prof["spmv_launches"])
+    flow_ms = prof["step_ms"] / max(1, prof["step_launches"])
+    step_launch_ms = infect_ms + flow_ms
     achieved = (bytes_replay / T) / (step_launch_ms / 1e3) / 1e9
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                        "frac": achieved / hbm, "peak_source": f"{peak_kind} (copy bandwidth)",
-                       "kernel": "k_step (one launch per step)",
+                       "kernel": "k_infect + k_flow (the two launches of one step)",
                        "algorithmic_bytes_per_launch": bytes_replay / T,
                        "avg_launch_us": step_launch_ms * 1e3,
+                       "avg_launch_us_by_kernel": {"k_infect": infect_ms * 1e3, "k_flow": flow_ms * 1e3},
                        "traffic": None}
     traffic, capture = profiled_traffic(args.workload)
     if traffic is not None:
@@ -397,14 +406,14 @@ def dense_stress_leg(replay_b200, dev, timed, hbm):
     nnz_total = pre.info["nnz_total"]
     pre.close()
     bytes_replay = algorithmic_bytes(n, M, T, nnz_total)
-    launch_ms = prof["step_ms"] / max(1, prof["step_launches"])
+    launch_ms = prof["spmv_ms"] / max(1, prof["spmv_launches"]) + prof["step_ms"] / max(1, prof["step_launches"])
     achieved = (bytes_replay / T) / (launch_ms / 1e3) / 1e9
     g.close()
     return {"workload": net["name"], "contacts": int(len(net["start"])), "ingest_s": ingest,
             "ms_per_replay": ms, "value": n * M * T / (ms / 1e3), "unit": UNIT,
             "nnz_per_step": nnz_total / T,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "kernel": "k_step", "algorithmic_bytes_per_launch": bytes_replay / T,
+                         "kernel": "k_infect + k_flow", "algorithmic_bytes_per_launch": bytes_replay / T,
                          "avg_launch_us": launch_ms * 1e3,
                          "note": "the 10 MB infectious mask stays in L2: algorithmic gather bytes exceed DRAM traffic"}}
 

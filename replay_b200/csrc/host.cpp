@@ -209,7 +209,8 @@ struct rp_sim {
   // plain state
   DevBuf state, exposure;
   // batched state
-  DevBuf sa, sb, mask, mask2, tasks, ev, rs, init_counts;
+  DevBuf sa, sb, mask, evs, flag, tasks, ev, rs, init_counts;
+  DevBuf mask2;  // countdown mode: the infectious masks alternate between steps
   DevBuf err;  // int32: set by a kernel that gave up a bounded wait
   // batched countdown state: per-replica codes into the countdown table
   DevBuf codes, cd_tab;
@@ -362,10 +363,12 @@ struct rp_sim {
       k += 2 + (p.initial_count > 0);
     } else {
       RP_TRY_CUDA(cudaMemsetAsync(ev.ptr, 0, ev.bytes, st));
+      // k_infect writes event words one by one; k_flow reads whole items
+      if (evs.ptr) RP_TRY_CUDA(cudaMemsetAsync(evs.ptr, 0, evs.bytes, st));
       if (rs.ptr && p.p_rs > 0.0f) RP_TRY_CUDA(cudaMemsetAsync(rs.ptr, 0, rs.bytes, st));
       RP_TRY_CUDA(cudaMemsetAsync(init_counts.ptr, 0, init_counts.bytes, st));
       packed_init(L, sa.as<uint32_t>(), sb.as<uint32_t>(), mask.as<uint32_t>(),
-                  p.initial_infected, p.initial_count, net_first.as<int32_t>(),
+                  flag.as<uint8_t>(), p.initial_infected, p.initial_count, net_first.as<int32_t>(),
                   net_rows.as<int32_t>(), n_nets, c, st);
       if (cd.code_bytes)  // countdown codes from the initial-infection plane
         cd_init(L, tasks.as<PackedTask>(), sa.as<uint32_t>(), codes.ptr, cd.code_bytes,
@@ -419,23 +422,30 @@ struct rp_sim {
         mark(kMarkStep);
         k += 2;
       } else {
-        // the infectious masks alternate: step t reads buffer t & 1 and
-        // writes every word of the other
-        const uint32_t *m_in = (t & 1) ? mask2.as<uint32_t>() : mask.as<uint32_t>();
-        uint32_t *m_out = (t & 1) ? mask.as<uint32_t>() : mask2.as<uint32_t>();
-        if (cd.code_bytes)
+        if (cd.code_bytes) {
+          // countdown codes: the infectious masks alternate, step t reads
+          // buffer t & 1 and writes every word of the other
+          const uint32_t *m_in = (t & 1) ? mask2.as<uint32_t>() : mask.as<uint32_t>();
+          uint32_t *m_out = (t & 1) ? mask.as<uint32_t>() : mask2.as<uint32_t>();
           cd_step(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t), m_in, m_out, codes.ptr,
                   cd.code_bytes, cd_tab.as<uint32_t>(), (int32_t)cd.tab.size(), cd.infect_code,
                   ev.as<unsigned long long>() + (int64_t)t * per_row, (uint32_t)t, c, st);
-        else
-          packed_step_fused(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t), m_in, m_out,
-                            sa.as<uint32_t>(), sb.as<uint32_t>(),
-                            ev.as<unsigned long long>() + (int64_t)t * per_row,
-                            p.p_rs > 0.0f ? rs.as<unsigned long long>() + (int64_t)t * per_row
-                                          : nullptr,
-                            (uint32_t)t, step_scale[t], c, st);
-        mark(kMarkStep);
-        k += 1;
+          mark(kMarkStep);
+          k += 1;
+        } else {
+          packed_infect(L, tasks.as<PackedTask>(), rp_of(t), ent_of(t), mask.as<uint32_t>(),
+                        sa.as<uint32_t>(), sb.as<uint32_t>(), evs.as<uint32_t>(),
+                        flag.as<uint8_t>(), (uint32_t)t, step_scale[t], c, st);
+          mark(kMarkSpmv);
+          packed_flow(L, tasks.as<PackedTask>(), rp_of(t), mask.as<uint32_t>(),
+                      sa.as<uint32_t>(), sb.as<uint32_t>(), evs.as<uint32_t>(),
+                      flag.as<uint8_t>(), ev.as<unsigned long long>() + (int64_t)t * per_row,
+                      p.p_rs > 0.0f ? rs.as<unsigned long long>() + (int64_t)t * per_row
+                                    : nullptr,
+                      (uint32_t)t, c, st);
+          mark(kMarkStep);
+          k += 2;
+        }
       }
       RP_TRY(emit_states(t + 1, step_ts[t]));
     }
@@ -738,14 +748,15 @@ rp_status alloc_state(rp_sim &s) {
   // network smaller than a task is one task); rp_sim_autotune refines them
   s.task_rows.assign(s.n_nets, rows_per_task(N, n_slices));
   RP_TRY(packed_prepare());
-  RP_TRY(step_prepare());
   RP_TRY(cd_prepare());
   const size_t plane = sizeof(uint32_t) * (size_t)N * L.words;
   RP_TRY(s.sa.alloc(plane));
   RP_TRY(s.sb.alloc(plane));
   RP_TRY(s.mask.alloc(plane));
-  RP_TRY(s.mask2.alloc(plane));
+  RP_TRY(s.flag.alloc(((size_t)N * L.q4 + 3) / 4 * 4));
+  if (!s.cd.code_bytes) RP_TRY(s.evs.alloc(plane));
   if (s.cd.code_bytes) {
+    RP_TRY(s.mask2.alloc(plane));
     RP_TRY(s.codes.alloc((size_t)s.cd.code_bytes * 32 * (size_t)N * L.words));
     RP_TRY(s.cd_tab.alloc(sizeof(uint32_t) * s.cd.tab.size()));
     RP_TRY_CUDA(cudaMemcpy(s.cd_tab.ptr, s.cd.tab.data(), sizeof(uint32_t) * s.cd.tab.size(),
@@ -1298,7 +1309,8 @@ RP_API rp_status rp_sim_get_info(const rp_sim *s, rp_sim_info *o) {
   o->prebuilt_nnz = s->prebuilt_nnz;
   int64_t bytes = 0;
   const DevBuf *bufs[] = {&s->arena_rp, &s->arena_ent, &s->state, &s->exposure, &s->sa,
-                          &s->sb, &s->mask, &s->mask2, &s->err, &s->codes, &s->cd_tab,
+                          &s->sb, &s->mask, &s->mask2, &s->evs, &s->flag, &s->err,
+                          &s->codes, &s->cd_tab,
                           &s->tasks, &s->ev, &s->rs,
                           &s->init_counts, &s->counts, &s->beta_r, &s->sus, &s->classes,
                           &s->wsp.hits, &s->wsp.entries, &s->wsp.erank, &s->wsp.tmp_e,

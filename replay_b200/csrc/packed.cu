@@ -1,15 +1,38 @@
-// Batched path, set-up and read-out kernels: initial conditions (Bernoulli
-// and exact-k seeding), full E/I/R counts of the planes, per-step counts
-// from the event rows, per-replica node classes, and the exposure test hook.
-// The per-step kernel is in step.cu.
+// Batched path: replica-bit-packed state, two kernels per step.
 //
 // Layout in HBM, node-major, 32 replicas per uint32 word; every node row is
-// padded to a multiple of 4 words (W words per node):
+// padded to a multiple of 4 words so that a lane moves 128 replicas with one
+// 16-byte access:
 //   sa, sb    state planes; replica bit (a, b): S (0,0), E (0,1), I (1,0),
 //             R (1,1)
-//   mask      infectious bits (a & ~b), two buffers alternating per step
-//   ev (+rs)  per-replica event counters of every step: S->E | ->I | I->
-//             in 21-bit fields (+ R->S), summed into counts by k_finalize
+//   mask      infectious bits (a & ~b); k_infect reads it, then k_flow
+//             rewrites the words whose state changed
+//   evs       infection events of the step (items with events only; a
+//             per-item flag byte tells k_flow which ones)
+// The window CSR holds {col, weight} pairs (int32 contact-seconds).
+//
+// k_infect (exposure SpMM + infection draws), per row with contacts, lanes
+// over 4-word columns (the replacement of cusparseSpMM,
+// tool/gpu_cpu_temporal_sim.cu:1062, and monte_carlo_simulation, :137-159):
+//   1. inf = OR over neighbours j of mask_t[j] (16 B per lane per entry);
+//   2. exposed = inf & S; the exposed replicas of a word compare the top
+//      byte of their infection uniforms (8 bit-sliced planes, two Philox
+//      calls per word) with that of the word bound B = max bs_r * e_max
+//      (e_max = the row's total contact-seconds, so every P <= B); only
+//      replicas at or below it compute their exact int64 exposure and
+//      P = 1 - exp(-beta_r s_i e) and finish the comparison against
+//      floor(P 2^64) (infect_event; the uniform's low 56 bits are drawn
+//      only on a tie of the top byte);
+//   3. events are OR-ed into evs and flag their item.
+// k_flow (transitions + count reduction), every (row, 4-word column):
+//   reads the planes and the row's infection events, draws the bit-sliced
+//   flow uniforms of the E, I (and waning R) replicas, 32 replicas per random
+//   plane (flow_events), applies all moves with bitwise operations, writes the
+//   planes and mask_{t+1}, and adds every transition event to per-replica
+//   counters in shared memory, flushed once per task to the step's event
+//   row; k_finalize turns initial counts + events into per-step counts.
+// Every decision uses the state at the start of the step: k_infect reads the
+// planes before k_flow rewrites them.
 #include "rp_device.cuh"
 #include "rp_internal.h"
 
@@ -19,11 +42,529 @@ namespace {
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kFieldBits = 21;  // global event fields: S->E | ->I | I->
 constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
 
 __device__ __forceinline__ uint32_t word_mask(const PackedLayout &L, int word) {
   return word < L.vwords - 1 ? kFull : (word == L.vwords - 1 ? L.last_mask : 0u);
 }
 
+__device__ __forceinline__ uint32_t get4(const uint4 &v, int w) {
+  return w == 0 ? v.x : (w == 1 ? v.y : (w == 2 ? v.z : v.w));
+}
+
+__device__ __forceinline__ void or4(uint4 &a, const uint4 b) {
+  a.x |= b.x;
+  a.y |= b.y;
+  a.z |= b.z;
+  a.w |= b.w;
+}
+
+// Fast division of an item index by the columns of a task (ncols <= 32,
+// items < 2^27): q = umulhi(i, ceil(2^32 / d)).
+struct Div {
+  uint32_t d, mag;
+  __device__ explicit Div(uint32_t dd) : d(dd), mag(dd > 1 ? 0xFFFFFFFFu / dd + 1u : 0u) {}
+  __device__ uint32_t div(uint32_t i) const { return d > 1 ? __umulhi(i, mag) : i; }
+};
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int &total) {
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  total = __shfl_sync(kFull, incl, 31);
+  return incl - v;
+}
+
+// Position of the k-th (from 0) set bit of t (k < popc(t)), by halving.
+__device__ __forceinline__ int nth_set_bit(uint32_t t, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    const int c = __popc(t & ((1u << w) - 1u));
+    if (k >= c) {
+      k -= c;
+      pos += w;
+      t >>= w;
+    }
+  }
+  return pos;
+}
+
+__device__ __forceinline__ int find_owner(const int32_t *off, int p) {
+  int owner = 0;
+#pragma unroll
+  for (int st = 16; st > 0; st >>= 1)
+    if (off[owner + st] <= p) owner += st;
+  return owner;
+}
+
+constexpr int kMaxTaskRows = 1024;  // rows of one task (host-side limit)
+
+constexpr int kEntCap = 768;        // staged CSR pairs per chunk
+constexpr int kEntBuf = kEntCap + 4; // a staging buffer (the copy may start one pair early)
+constexpr int kPiece = kEntBuf / 2 - 2;  // pairs per piece of a long row (a half buffer)
+constexpr long long kSpinLimit = 1ll << 22;
+
+// ---- bulk asynchronous copies (global -> this CTA's shared memory) ----------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+}
+// Waits for the phase with the given parity to complete; false after
+// kSpinLimit polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long long i = 0; i < kSpinLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// Stages pairs [k0, k1) of `ent` (k1 - k0 <= kEntBuf - 2) into `dst` with one
+// bulk copy (cp.async.bulk, no multicast) completing on `bar`; the copy
+// starts on the 16-byte boundary at or below pair k0, so pair k lands at
+// dst[k - k0 + shift].  Returns shift.  Issued by one thread.
+__device__ __forceinline__ int stage_pairs(int2 *dst, const int2 *ent, int32_t k0, int32_t k1,
+                                           unsigned long long *bar) {
+  const uintptr_t src = reinterpret_cast<uintptr_t>(ent + k0);
+  const int shift = (int)((src & 15u) >> 3);
+  const uint32_t bytes = ((uint32_t)(k1 - k0 + shift) * 8u + 15u) & ~15u;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(ent + k0 - shift), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+  return shift;
+}
+__device__ __forceinline__ int pair_shift(const int2 *ent, int32_t k0) {
+  return (int)((reinterpret_cast<uintptr_t>(ent + k0) & 15u) >> 3);
+}
+
+// ---------------------------------------------------------------------------
+// Per-warp queue of exposed words of k_infect (dynamic shared memory):
+// entries accumulate over rows and are decided 32 at a time.
+constexpr int kInfectQueue = 160;  // 31 left over + 4 words x 32 lanes of one pass
+struct InfectQueue {
+  uint4 pl[32][2];               // the 8 random planes of each word (round scratch)
+  int32_t rloc[kInfectQueue];    // task-relative row
+  int32_t word[kInfectQueue];    // word index within the row
+  uint32_t X[kInfectQueue];      // exposed replicas of the word
+  float efmax[kInfectQueue];     // ef(e_max) of the row
+  uint32_t C[32];      // candidates after the bound test (round scratch)
+  int32_t off[32];     // warp scan offsets of the candidates
+  // candidates carried to the next round (fewer than 32), self-contained
+  int32_t krloc[32];
+  int32_t kwb[32];  // word << 5 | replica bit
+  uint8_t ku8[32];  // top 8 bits of the replica's uniform
+  // exact-test batch: per candidate lane, its row's first CSR pair, its
+  // word << 5 | bit, the scan offsets of the batch's (candidate, pair)
+  // products and the exposure sums
+  int32_t cbeg[32];
+  int32_t cword[32];
+  int32_t poff[32];
+  long long esum[32];
+  int32_t n;
+  int32_t nk;
+};
+
+constexpr int kInfectDynSmem = 2 * kEntBuf * 8 + 128 * 32 * 4 + kWarps * (int)sizeof(InfectQueue);
+
+// Top 8 uniform bits of replica bit b from a queued word's planes.
+__device__ __forceinline__ uint32_t queued_top8(const uint4 (&q)[2], uint32_t b) {
+  const uint4 a = q[0], c = q[1];
+  const uint32_t pl[8] = {a.x, a.y, a.z, a.w, c.x, c.y, c.z, c.w};
+  return top8_of(pl, b);
+}
+
+// Decides up to 32 queued exposed words: the bound test one word per lane
+// (phase 2), then the exact test of the surviving candidates one replica
+// per lane (phase 3), in full batches of 32 together with the candidates
+// carried from earlier rounds; fewer than 32 left over are carried to the
+// next round unless `drain` is set.  Events are OR-ed into their words and
+// flag their items.
+__device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, int lane,
+                                             const PackedLayout &L, const PackedTask &T,
+                                             int cbase, const int32_t *s_rp, const int2 *s_ent,
+                                             const int2 *__restrict__ ent, bool staged,
+                                             int32_t e0, const float *s_beta, const float *s_bw,
+                                             const uint32_t *mask_w, uint32_t *evs_w,
+                                             uint32_t *flag32, uint32_t step, float scale,
+                                             const StepConsts &c) {
+  // ---- phase 2: bound test, one word per lane ----
+  uint32_t Cw = 0;
+  if (lane < n) {
+    const int orow = T.row_begin + Q.rloc[lane];
+    const int word = Q.word[lane];
+    // every exposed replica has P <= x <= |bs_r| ef(e_max) =: B; replicas
+    // whose uniform's top byte is above B's cannot infect
+    float bsmax = c.beta_r ? s_bw[word - 4 * cbase] : fabsf(c.beta);
+    if (c.sus) bsmax = __fmul_rn(bsmax, fabsf(c.sus[orow]));
+    const float B = __fmul_rn(bsmax, Q.efmax[lane]);
+    if (B > 0.0f) {
+      uint32_t pl[8];
+      infect_planes(c.rk, (uint32_t)orow, step, (uint32_t)word + (c.roff >> 5), pl);
+      Cw = B >= 1.0f ? Q.X[lane] : top8_le(Q.X[lane], fixed64(B), pl);
+      Q.pl[lane][0] = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+      Q.pl[lane][1] = make_uint4(pl[4], pl[5], pl[6], pl[7]);
+    }
+  }
+  Q.C[lane] = Cw;
+  int ctotal;
+  Q.off[lane] = warp_excl_scan(__popc(Cw), lane, ctotal);
+  __syncwarp();
+  // ---- phase 3: exact test of 32 candidates at a time ----
+  // The batch's (candidate, CSR pair) products are spread over the lanes:
+  // every pair is one independent mask-word load (a long row is shared by
+  // all 32 lanes), and the exposures sum in shared memory (exact int64).
+  const int nk = Q.nk;
+  const int total = nk + ctotal;
+  int base = 0;
+  for (; total - base >= 32 || (drain && base < total); base += 32) {
+    const int p = base + lane;
+    int orl = 0, word = 0, b = 0, npairs = 0;
+    int32_t beg = 0;
+    uint32_t u8 = 0;
+    if (p < total) {
+      if (p < nk) {
+        const int wb = Q.kwb[p];
+        orl = Q.krloc[p];
+        word = wb >> 5;
+        b = wb & 31;
+        u8 = Q.ku8[p];
+      } else {
+        const int o = find_owner(Q.off, p - nk);
+        b = nth_set_bit(Q.C[o], p - nk - Q.off[o]);
+        orl = Q.rloc[o];
+        word = Q.word[o];
+        u8 = queued_top8(Q.pl[o], (uint32_t)b);
+      }
+      beg = s_rp[orl];
+      npairs = s_rp[orl + 1] - beg;
+    }
+    int ptotal;
+    const int poff = warp_excl_scan(npairs, lane, ptotal);
+    __syncwarp();
+    Q.poff[lane] = poff;
+    Q.cbeg[lane] = beg;
+    Q.cword[lane] = word << 5 | b;
+    Q.esum[lane] = 0;
+    __syncwarp();
+    for (int q0 = 0; q0 < ptotal; q0 += 64) {
+      int32_t pc[2], pw[2], cw[2], own[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int q = q0 + 32 * h + lane;
+        own[h] = -1;
+        pc[h] = pw[h] = cw[h] = 0;
+        if (q < ptotal) {
+          const int o = find_owner(Q.poff, q);
+          const int32_t k = Q.cbeg[o] + (q - Q.poff[o]);
+          const int2 e = staged ? s_ent[k - e0] : __ldg(ent + k);
+          pc[h] = e.x;
+          pw[h] = e.y;
+          cw[h] = Q.cword[o];
+          own[h] = o;
+        }
+      }
+      uint32_t mw[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        mw[h] = own[h] >= 0 ? mask_w[(int64_t)pc[h] * L.words + (cw[h] >> 5)] : 0u;
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        if (own[h] >= 0 && ((mw[h] >> (cw[h] & 31)) & 1u))
+          atomicAdd(reinterpret_cast<unsigned long long *>(&Q.esum[own[h]]),
+                    (unsigned long long)(long long)pw[h]);
+    }
+    __syncwarp();
+    if (p >= total) continue;
+    const int orow = T.row_begin + orl;
+    const long long e = Q.esum[lane];
+    const float br = c.beta_r ? s_beta[(word - 4 * cbase) * 32 + b] : c.beta;
+    const float bs = c.sus ? __fmul_rn(br, c.sus[orow]) : br;
+    float ef = __ll2float_rn(e);
+    if (scale != 1.0f) ef = __fmul_rn(ef, scale);
+    const float xx = __fmul_rn(bs, ef);
+    if (!(xx > 0.0f)) continue;
+    // P <= x: a uniform whose top byte is above x's cannot infect (no
+    // exponential)
+    if (xx < 1.0f && u8 > (uint32_t)(fixed64(xx) >> 56)) continue;
+    const uint32_t gword = (uint32_t)word + (c.roff >> 5);
+    if (infect_event(one_minus_exp_neg(xx), u8, c.rk, (uint32_t)orow, step,
+                     gword * 32u + (uint32_t)b)) {
+      atomicOr(&evs_w[(int64_t)orow * L.words + word], 1u << b);
+      const int64_t idx = (int64_t)orow * L.q4 + (word >> 2);
+      atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
+    }
+  }
+  __syncwarp();
+  // carry the rest: slots below nk keep their entries when no batch ran
+  const int rest = total - base;
+  if (rest > 0) {
+    const int p = base + lane;
+    if (p < total && p >= nk) {
+      const int o = find_owner(Q.off, p - nk);
+      const int b = nth_set_bit(Q.C[o], p - nk - Q.off[o]);
+      Q.kwb[lane] = Q.word[o] << 5 | b;
+      Q.krloc[lane] = Q.rloc[o];
+      Q.ku8[lane] = (uint8_t)queued_top8(Q.pl[o], (uint32_t)b);
+    }
+  }
+  __syncwarp();
+  if (lane == 0) Q.nk = rest > 0 ? rest : 0;
+  __syncwarp();
+}
+
+// One item (row, 4-word column) per lane gathers the OR of the neighbours'
+// mask words (its loads issued together) and queues its exposed words;
+// infect_round decides the queue 32 words at a time, so that every lane
+// works on a dense list of words and then of candidate replicas.
+__global__ void __launch_bounds__(kThreads, 3)
+    k_infect(PackedLayout L, const PackedTask *__restrict__ tasks,
+             const int32_t *__restrict__ row_ptr, const int2 *__restrict__ ent,
+             const uint4 *__restrict__ mask_in, const uint4 *__restrict__ sa,
+             const uint4 *__restrict__ sb, uint4 *__restrict__ evs,
+             uint32_t *__restrict__ flag32, uint32_t step, float scale, StepConsts c) {
+  __shared__ int32_t s_rp[kMaxTaskRows + 1];
+  __shared__ float s_bw[128];  // max |beta_r| of each word of the slice
+  __shared__ uint4 s_lor[32];  // long row: OR of the neighbours' masks per column
+  __shared__ long long s_lemax;
+  __shared__ unsigned long long s_bar[4];  // chunk buffers 0, 1; long-row halves 0, 1
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  int2 *const s_buf0 = reinterpret_cast<int2 *>(s_dyn);  // two staging buffers of kEntBuf pairs
+  auto bufp = [&](int b) { return s_buf0 + b * kEntBuf; };
+  float *s_beta = reinterpret_cast<float *>(s_dyn + 2 * kEntBuf * sizeof(int2));
+  InfectQueue &Q = reinterpret_cast<InfectQueue *>(
+      s_dyn + 2 * kEntBuf * sizeof(int2) + 128 * 32 * sizeof(float))[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t *mask_w = reinterpret_cast<const uint32_t *>(mask_in);
+  uint32_t *evs_w = reinterpret_cast<uint32_t *>(evs);
+  if (lane == 0) {
+    Q.n = 0;
+    Q.nk = 0;
+  }
+  if (threadIdx.x < 4) mbar_init(&s_bar[threadIdx.x]);
+  if (threadIdx.x == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncthreads();
+  uint32_t cph = 0, pph = 0;  // phase parity of each chunk buffer / half barrier
+  int buf = 0;
+  // every thread waits on the same barriers in the same order; a wait that
+  // gives up raises the error flag (the host fails the run)
+  auto wait_bar = [&](int b, uint32_t &ph, int bit) {
+    const bool ready = mbar_wait(&s_bar[b], (ph >> bit) & 1u);
+    ph ^= 1u << bit;
+    if (!ready && c.err) atomicExch(c.err, 1);
+  };
+  for (int ti = blockIdx.x; ti < L.n_tasks; ti += gridDim.x) {
+    const PackedTask T = tasks[ti];
+    const int cbase = T.slice * 32;
+    const int ncols = min(32, L.q4 - cbase);
+    const Div dv((uint32_t)ncols);
+    const int nrows = T.row_end - T.row_begin;
+    for (int i = threadIdx.x; i <= nrows; i += blockDim.x) s_rp[i] = row_ptr[T.row_begin + i];
+    if (c.beta_r) {
+      for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x)
+        s_beta[j] = cbase * 128 + j < L.m ? c.beta_r[cbase * 128 + j] : 0.0f;
+      __syncthreads();
+      for (int wl = threadIdx.x; wl < ncols * 4; wl += blockDim.x) {
+        float mx = 0.0f;
+        for (int r = 0; r < 32; ++r) mx = fmaxf(mx, fabsf(s_beta[wl * 32 + r]));
+        s_bw[wl] = mx;
+      }
+    }
+    __syncthreads();
+    // chunk of rows [r0, end) whose CSR pairs fit a staging buffer (>= 1 row)
+    auto chunk_end = [&](int r0) {
+      int lo = r0 + 1, hi = nrows;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_rp[mid] - s_rp[r0] <= kEntCap) lo = mid; else hi = mid - 1;
+      }
+      return lo;
+    };
+    // the chunk's pairs go to buffer b with one bulk copy (thread 0)
+    auto stage_chunk = [&](int ra, int rb, int b) {
+      const int32_t k0 = s_rp[ra], k1 = s_rp[rb];
+      if (threadIdx.x == 0 && k1 > k0 && k1 - k0 <= kEntCap)
+        stage_pairs(bufp(b), ent, k0, k1, &s_bar[b]);
+    };
+    int r0 = 0, r1 = nrows > 0 ? chunk_end(0) : 0;
+    if (nrows > 0) stage_chunk(0, r1, buf);
+    while (r0 < nrows) {
+      const int r2 = r1 < nrows ? chunk_end(r1) : nrows;
+      if (r1 < nrows) stage_chunk(r1, r2, buf ^ 1);  // prefetch the next chunk's pairs
+      const int32_t e0 = s_rp[r0], e1 = s_rp[r1];
+      const bool staged = e1 - e0 <= kEntCap;
+      if (staged && e1 > e0) wait_bar(buf, cph, buf);
+      const int2 *s_ent = bufp(buf) + pair_shift(ent, e0);
+      const bool long_row = !staged;  // one row with more pairs than a buffer
+      if (long_row) {
+        // its pairs stream through the two halves of this chunk's buffer, one
+        // piece ahead; every warp ORs the neighbours' mask words of its share
+        // of a piece (lane = column) and the shares combine in shared memory
+        int2 *const half0 = bufp(buf);
+        auto half = [&](int h) { return half0 + h * (kEntBuf / 2); };
+        if (threadIdx.x < 32) s_lor[threadIdx.x] = make_uint4(0, 0, 0, 0);
+        if (threadIdx.x == 0) {
+          s_lemax = 0;
+          stage_pairs(half(0), ent, e0, min(e0 + kPiece, e1), &s_bar[2]);
+        }
+        uint4 linf = make_uint4(0, 0, 0, 0);
+        long long lemax = 0;
+        const int npieces = (e1 - e0 + kPiece - 1) / kPiece;
+        for (int pk = 0; pk < npieces; ++pk) {
+          const int hb = pk & 1;
+          const int32_t p0 = e0 + pk * kPiece, p1 = min(p0 + kPiece, e1);
+          if (threadIdx.x == 0 && pk + 1 < npieces)
+            stage_pairs(half(hb ^ 1), ent, p1, min(p1 + kPiece, e1), &s_bar[2 + (hb ^ 1)]);
+          wait_bar(2 + hb, pph, hb);
+          const int2 *pc = half(hb) + pair_shift(ent, p0);
+          int32_t k = p0 + warp;
+          for (; k + 3 * kWarps < p1; k += 4 * kWarps) {
+            const int2 q0 = pc[k - p0], q1 = pc[k - p0 + kWarps], q2 = pc[k - p0 + 2 * kWarps],
+                       q3 = pc[k - p0 + 3 * kWarps];
+            if (lane < ncols) {
+              const uint4 m0 = mask_in[(int64_t)q0.x * L.q4 + cbase + lane];
+              const uint4 m1 = mask_in[(int64_t)q1.x * L.q4 + cbase + lane];
+              const uint4 m2 = mask_in[(int64_t)q2.x * L.q4 + cbase + lane];
+              const uint4 m3 = mask_in[(int64_t)q3.x * L.q4 + cbase + lane];
+              or4(linf, m0);
+              or4(linf, m1);
+              or4(linf, m2);
+              or4(linf, m3);
+            }
+            lemax += (long long)q0.y + q1.y + q2.y + q3.y;
+          }
+          for (; k < p1; k += kWarps) {
+            const int2 q0 = pc[k - p0];
+            if (lane < ncols) or4(linf, mask_in[(int64_t)q0.x * L.q4 + cbase + lane]);
+            lemax += q0.y;
+          }
+          __syncthreads();  // the half is free to restage
+        }
+        if (lane < ncols) {
+          atomicOr(&s_lor[lane].x, linf.x);
+          atomicOr(&s_lor[lane].y, linf.y);
+          atomicOr(&s_lor[lane].z, linf.z);
+          atomicOr(&s_lor[lane].w, linf.w);
+        }
+        if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long *>(&s_lemax),
+                                 (unsigned long long)lemax);
+        __syncthreads();
+      }
+      const int nitems = (r1 - r0) * ncols;
+      // warp-uniform; one pass past the items decides what is left queued
+      // (the staged pairs change with the next chunk)
+      for (int it0 = warp * 32;; it0 += kWarps * 32) {
+        const bool flushing = it0 >= nitems;
+        // ---- phase 1: gather, per lane ----
+        const int it = it0 + lane;
+        const bool ok = it < nitems;
+        const int rl = ok ? (int)dv.div((uint32_t)it) : 0;
+        const int cc = ok ? it - rl * ncols : 0;
+        const int rloc = r0 + rl;
+        const int col = cbase + cc;
+        const int row = T.row_begin + rloc;
+        const int32_t beg = s_rp[rloc], end = s_rp[rloc + 1];
+        const int n = ok ? end - beg : 0;
+        uint32_t X[4] = {0, 0, 0, 0};
+        float efmax = 0.0f;
+        if (n > 0) {
+          const int64_t idx = (int64_t)row * L.q4 + col;
+          const uint4 a4 = sa[idx], b4 = sb[idx];
+          const int2 *er = s_ent + (beg - e0);
+          uint4 inf = make_uint4(0, 0, 0, 0);
+          long long emax = 0;
+          int k = 0;
+          if (long_row) {  // gathered by the whole CTA above
+            inf = s_lor[cc];
+            emax = s_lemax;
+            k = n;
+          }
+          for (; k + 4 <= n; k += 4) {
+            const int2 q0 = er[k], q1 = er[k + 1], q2 = er[k + 2], q3 = er[k + 3];
+            const uint4 m0 = mask_in[(int64_t)q0.x * L.q4 + col];
+            const uint4 m1 = mask_in[(int64_t)q1.x * L.q4 + col];
+            const uint4 m2 = mask_in[(int64_t)q2.x * L.q4 + col];
+            const uint4 m3 = mask_in[(int64_t)q3.x * L.q4 + col];
+            or4(inf, m0);
+            or4(inf, m1);
+            or4(inf, m2);
+            or4(inf, m3);
+            emax += (long long)q0.y + q1.y + q2.y + q3.y;
+          }
+          for (; k < n; ++k) {
+            const int2 q0 = er[k];
+            or4(inf, mask_in[(int64_t)q0.x * L.q4 + col]);
+            emax += q0.y;
+          }
+#pragma unroll
+          for (int w = 0; w < 4; ++w)
+            X[w] = get4(inf, w) & ~get4(a4, w) & ~get4(b4, w) & word_mask(L, 4 * col + w);
+          efmax = __ll2float_rn(emax);
+          if (scale != 1.0f) efmax = __fmul_rn(efmax, scale);
+        }
+        // ---- queue the exposed words ----
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const unsigned qm = __ballot_sync(kFull, X[w] != 0u);
+          if (!qm) continue;
+          const int base = Q.n;
+          if (X[w]) {
+            const int pos = base + __popc(qm & ((1u << lane) - 1u));
+            Q.rloc[pos] = rloc;
+            Q.word[pos] = 4 * col + w;
+            Q.X[pos] = X[w];
+            Q.efmax[pos] = efmax;
+          }
+          __syncwarp();
+          if (lane == 0) Q.n = base + __popc(qm);
+          __syncwarp();
+        }
+        // ---- decide full rounds (and, past the items, the remainder and
+        // the carried candidates: the staged pairs change with the chunk) ----
+        while (Q.n >= 32 || (flushing && (Q.n > 0 || Q.nk > 0))) {
+          const int take = Q.n < 32 ? Q.n : 32;
+          infect_round(Q, take, flushing && take == Q.n, lane, L, T, cbase, s_rp, s_ent, ent,
+                       staged, e0, s_beta, s_bw, mask_w, evs_w, flag32, step, scale, c);
+          const int rest = Q.n - take;
+          for (int i = lane; i < rest; i += 32) {
+            Q.rloc[i] = Q.rloc[take + i];
+            Q.word[i] = Q.word[take + i];
+            Q.X[i] = Q.X[take + i];
+            Q.efmax[i] = Q.efmax[take + i];
+          }
+          __syncwarp();
+          if (lane == 0) Q.n = rest;
+          __syncwarp();
+        }
+        if (flushing) break;
+      }
+      __syncthreads();
+      r0 = r1;
+      r1 = r2;
+      buf ^= 1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 __device__ __forceinline__ void count_bits(unsigned long long *s_ev, int wl, uint32_t t,
                                            unsigned long long inc) {
   while (t) {
@@ -33,6 +574,226 @@ __device__ __forceinline__ void count_bits(unsigned long long *s_ev, int wl, uin
   }
 }
 
+// Applies one word's moves; returns the new planes and counts the events.
+__device__ __forceinline__ void apply_word(uint32_t A, uint32_t B, uint32_t evS, uint32_t f,
+                                           bool waning, const StepConsts &c,
+                                           unsigned long long *s_ev, int wl, uint32_t &na,
+                                           uint32_t &nb) {
+  const uint32_t E = ~A & B, I = A & ~B, Rw = waning ? (A & B) : 0u;
+  const uint32_t evE = f & E, evI = f & I, evR = f & Rw;
+  uint32_t xa = A, xb = B;
+  if (c.has_exposed)
+    xb |= evS;
+  else
+    xa |= evS;
+  xa |= evE;
+  xb &= ~evE;
+  if (c.ir_to_s)
+    xa &= ~evI;
+  else
+    xb |= evI;
+  xa &= ~evR;
+  xb &= ~evR;
+  na = xa;
+  nb = xb;
+  if (evS | evE | evI | evR) {
+    count_bits(s_ev, wl, c.has_exposed ? evS : 0u, 1ull);
+    count_bits(s_ev, wl, evE | (c.has_exposed ? 0u : evS), 1ull << 16);
+    count_bits(s_ev, wl, evI, 1ull << 32);
+    count_bits(s_ev, wl, evR, 1ull << 48);
+  }
+}
+
+// Per-warp queue of words with flow candidates (dynamic shared memory):
+// words are queued while the warp streams its items and drawn in full
+// 32-lane rounds, so sparse candidates do not leave lanes idle.
+constexpr int kFlowIPL = 4;      // items per lane per pass (loads in flight)
+constexpr int kFlowQueue = 576;  // 31 left over + 4 words x kFlowIPL items x 32 lanes (+ pad)
+struct FlowQueue {
+  int32_t row[kFlowQueue];
+  uint16_t word[kFlowQueue];  // word index within the row
+  int32_t n;
+};
+constexpr int kFlowDynSmem = 128 * 32 * 8 + kWarps * (int)sizeof(FlowQueue);
+
+// Draws the flows of queue entries [0, cnt) (cnt <= 32, one per lane) and
+// writes the words: infection events and flows act on disjoint state bits,
+// so both are applied here from the start-of-step planes.
+__device__ __forceinline__ void flow_round(const FlowQueue &Q, int base, int cnt, int lane,
+                                           bool waning, const StepConsts &c, uint32_t step,
+                                           unsigned long long *s_ev, uint32_t *sa_w,
+                                           uint32_t *sb_w, uint32_t *mask_w, uint32_t *evs_w,
+                                           int words, int cbase) {
+  if (lane < cnt) {
+    const int q = base + lane;
+    const int row = Q.row[q], word = Q.word[q];
+    const int64_t wi = (int64_t)row * words + word;
+    const uint32_t A = sa_w[wi], B = sb_w[wi], ev = evs_w[wi];
+    if (ev) evs_w[wi] = 0u;
+    const uint32_t E = ~A & B, I = A & ~B, R = waning ? (A & B) : 0u;
+    const uint32_t f =
+        flow_events(E, I, R, c.th, c.rk, (uint32_t)row, step, (uint32_t)word + (c.roff >> 5));
+    uint32_t na, nb;
+    apply_word(A, B, ev, f, waning, c, s_ev, word - 4 * cbase, na, nb);
+    if (na != A || nb != B) {
+      sa_w[wi] = na;
+      sb_w[wi] = nb;
+      mask_w[wi] = na & ~nb;
+    }
+  }
+}
+
+// Streams the items of each task: infection events of words without flow
+// candidates are applied on the spot, words with candidates are queued.
+__global__ void __launch_bounds__(kThreads, 3)
+    k_flow(PackedLayout L, const PackedTask *__restrict__ tasks,
+           const int32_t *__restrict__ row_ptr, uint4 *__restrict__ evs,
+           uint4 *__restrict__ mask, uint4 *__restrict__ sa, uint4 *__restrict__ sb,
+           uint8_t *__restrict__ flag, unsigned long long *__restrict__ ev_row,
+           unsigned long long *__restrict__ rs_row, uint32_t step, StepConsts c) {
+  extern __shared__ __align__(16) unsigned char s_dynf[];
+  // 4 x 16-bit event counters per replica of the slice
+  unsigned long long *s_ev = reinterpret_cast<unsigned long long *>(s_dynf);
+  FlowQueue &Q = reinterpret_cast<FlowQueue *>(s_dynf + 128 * 32 * 8)[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool waning = c.th.tr_all || c.th.tr != 0;
+  uint32_t *sa_w = reinterpret_cast<uint32_t *>(sa);
+  uint32_t *sb_w = reinterpret_cast<uint32_t *>(sb);
+  uint32_t *mask_w = reinterpret_cast<uint32_t *>(mask);
+  for (int ti = blockIdx.x; ti < L.n_tasks; ti += gridDim.x) {
+    const PackedTask T = tasks[ti];
+    const int cbase = T.slice * 32;
+    const int ncols = min(32, L.q4 - cbase);
+    const Div dv((uint32_t)ncols);
+    const int nrows = T.row_end - T.row_begin;
+    for (int j = threadIdx.x; j < 128 * 32; j += blockDim.x) s_ev[j] = 0;
+    if (lane == 0) Q.n = 0;
+    __syncthreads();
+    const int nitems = nrows * ncols;
+    uint32_t *evs_w = reinterpret_cast<uint32_t *>(evs);
+    // warp-uniform passes of kFlowIPL items per lane, all loads issued
+    // first; candidate words are queued, and full rounds of 32 decided after
+    // the pass (one pass past the items decides the rest; one call site of
+    // flow_round keeps the kernel small)
+    for (int it0 = warp * 32 * kFlowIPL;; it0 += kWarps * 32 * kFlowIPL) {
+      const bool flushing = it0 >= nitems;
+      int rl[kFlowIPL], cl[kFlowIPL];
+      bool in[kFlowIPL];
+      uint8_t st[kFlowIPL];
+      uint4 a4[kFlowIPL], b4[kFlowIPL];
+#pragma unroll
+      for (int h = 0; h < kFlowIPL; ++h) {
+        const int itv = it0 + 32 * h + lane;
+        in[h] = itv < nitems;
+        rl[h] = in[h] ? (int)dv.div((uint32_t)itv) : 0;
+        cl[h] = in[h] ? itv - rl[h] * ncols : 0;
+        const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
+        a4[h] = b4[h] = make_uint4(0, 0, 0, 0);
+        st[h] = 0;
+        if (in[h]) {
+          st[h] = flag[idx];
+          a4[h] = sa[idx];
+          b4[h] = sb[idx];
+        }
+      }
+      // quiet items (every replica susceptible, or recovered without waning,
+      // and no infection event) need no work: skip them a warp at a time
+      bool busy = false;
+      uint32_t cm[kFlowIPL];
+      int cnt = 0;
+#pragma unroll
+      for (int h = 0; h < kFlowIPL; ++h) {
+        cm[h] = 0;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const uint32_t A = get4(a4[h], w), B = get4(b4[h], w);
+          const bool valid = in[h] && word_mask(L, 4 * (cbase + cl[h]) + w) != 0u;
+          if (valid && (waning ? (A | B) : (A ^ B)) != 0u) cm[h] |= 1u << w;
+        }
+        cnt += __popc(cm[h]);
+        busy |= st[h] != 0 || cm[h] != 0;
+      }
+      if (!flushing && !__any_sync(kFull, busy)) continue;
+      // infection events: words without flow candidates are applied here;
+      // the queued words' events are read (and cleared) by their round
+#pragma unroll
+      for (int h = 0; h < kFlowIPL; ++h) {
+        if (!st[h]) continue;
+        const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
+        const uint4 e4 = evs[idx];
+        flag[idx] = 0;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const uint32_t ev = get4(e4, w);
+          if (!ev || ((cm[h] >> w) & 1u)) continue;
+          const int word = 4 * (cbase + cl[h]) + w;
+          const int64_t wi = (int64_t)(T.row_begin + rl[h]) * L.words + word;
+          uint32_t na, nb;
+          apply_word(get4(a4[h], w), get4(b4[h], w), ev, 0u, waning, c, s_ev, 4 * cl[h] + w, na,
+                     nb);
+          sa_w[wi] = na;
+          sb_w[wi] = nb;
+          mask_w[wi] = na & ~nb;
+          evs_w[wi] = 0u;
+        }
+      }
+      // queue the candidate words of the pass (one scan)
+      int total;
+      int pos = warp_excl_scan(cnt, lane, total);
+      if (total > 0) {  // warp-uniform
+        pos += Q.n;
+#pragma unroll
+        for (int h = 0; h < kFlowIPL; ++h)
+#pragma unroll
+          for (int w = 0; w < 4; ++w)
+            if ((cm[h] >> w) & 1u) {
+              Q.row[pos] = T.row_begin + rl[h];
+              Q.word[pos] = (uint16_t)(4 * (cbase + cl[h]) + w);
+              ++pos;
+            }
+        __syncwarp();
+      }
+      const int n = Q.n + total;
+      int start = 0;
+      for (; n - start >= 32 || (flushing && n - start > 0); start += 32)
+        flow_round(Q, start, min(32, n - start), lane, waning, c, step, s_ev, sa_w, sb_w, mask_w,
+                   evs_w, L.words, cbase);
+      __syncwarp();
+      const int rest = max(n - start, 0);
+      if (start > 0 && rest > 0) {  // move the remainder (< 32 words) to the front
+        const int q = start + lane;
+        int32_t r0 = 0;
+        uint16_t w0 = 0;
+        if (lane < rest) {
+          r0 = Q.row[q];
+          w0 = Q.word[q];
+        }
+        __syncwarp();
+        if (lane < rest) {
+          Q.row[lane] = r0;
+          Q.word[lane] = w0;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) Q.n = rest;
+      __syncwarp();
+      if (flushing) break;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x) {
+      const unsigned long long v = s_ev[j];
+      if (!v) continue;
+      const int rep = cbase * 128 + j;
+      if (rep >= L.m) continue;
+      const unsigned long long f16 = 0xFFFFull;
+      const unsigned long long g = (v & f16) | (((v >> 16) & f16) << kFieldBits) |
+                                   (((v >> 32) & f16) << (2 * kFieldBits));
+      if (g) atomicAdd(&ev_row[T.count_base + rep], g);
+      if (rs_row && (v >> 48)) atomicAdd(&rs_row[T.count_base + rep], v >> 48);
+    }
+    __syncthreads();
+  }
+}
 // Full E/I/R counts of the planes (initial state): one shared atomic per
 // set bit, E | I << 21 | R << 42 per replica.
 __global__ void __launch_bounds__(kThreads)
@@ -200,10 +961,17 @@ int task_grid(int n_tasks, int per_sm) {
 
 }  // namespace
 
-rp_status packed_prepare() { return RP_OK; }
+rp_status packed_prepare() {
+  cudaError_t e = cudaFuncSetAttribute(k_flow, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kFlowDynSmem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_flow)");
+  e = cudaFuncSetAttribute(k_infect, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfectDynSmem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_infect)");
+  return RP_OK;
+}
 
 void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb, uint32_t *mask,
-                 float p0, int32_t k_exact, const int32_t *net_first_row,
+                 uint8_t *flag, float p0, int32_t k_exact, const int32_t *net_first_row,
                  const int32_t *net_rows, int32_t n_nets, const StepConsts &c,
                  cudaStream_t st) {
   const int64_t total = (int64_t)L.n_nodes * L.words;
@@ -214,6 +982,35 @@ void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb, uint32_t *ma
                                                                 n_nets, k_exact, c);
     k_mask_from_planes<<<1184, 256, 0, st>>>(total, sa, sb, mask);
   }
+  cudaMemsetAsync(flag, 0, ((size_t)L.n_nodes * L.q4 + 3) / 4 * 4, st);
+}
+
+void packed_step(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
+                 const int2 *entries, uint32_t *mask, uint32_t *sa, uint32_t *sb, uint32_t *evs,
+                 uint8_t *flag, unsigned long long *ev_row, unsigned long long *rs_row,
+                 uint32_t step, float scale, const StepConsts &c, cudaStream_t st) {
+  packed_infect(L, tasks, row_ptr, entries, mask, sa, sb, evs, flag, step, scale, c, st);
+  packed_flow(L, tasks, row_ptr, mask, sa, sb, evs, flag, ev_row, rs_row, step, c, st);
+}
+
+void packed_infect(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
+                   const int2 *entries, const uint32_t *mask, const uint32_t *sa,
+                   const uint32_t *sb, uint32_t *evs, uint8_t *flag, uint32_t step, float scale,
+                   const StepConsts &c, cudaStream_t st) {
+  k_infect<<<task_grid(L.n_tasks, 3), kThreads, kInfectDynSmem, st>>>(
+      L, tasks, row_ptr, entries, reinterpret_cast<const uint4 *>(mask),
+      reinterpret_cast<const uint4 *>(sa), reinterpret_cast<const uint4 *>(sb),
+      reinterpret_cast<uint4 *>(evs), reinterpret_cast<uint32_t *>(flag), step, scale, c);
+}
+
+void packed_flow(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
+                 uint32_t *mask, uint32_t *sa, uint32_t *sb, const uint32_t *evs, uint8_t *flag,
+                 unsigned long long *ev_row, unsigned long long *rs_row, uint32_t step,
+                 const StepConsts &c, cudaStream_t st) {
+  k_flow<<<task_grid(L.n_tasks, 3), kThreads, kFlowDynSmem, st>>>(
+      L, tasks, row_ptr, reinterpret_cast<uint4 *>(const_cast<uint32_t *>(evs)),
+      reinterpret_cast<uint4 *>(mask), reinterpret_cast<uint4 *>(sa),
+      reinterpret_cast<uint4 *>(sb), flag, ev_row, rs_row, step, c);
 }
 
 void packed_count(const PackedLayout &L, const PackedTask *tasks, const uint32_t *sa,

@@ -60,6 +60,35 @@ __device__ __forceinline__ void philox4x32_10_rk(uint32_t c0, uint32_t c1, uint3
   out[3] = c3;
 }
 
+// Two independent calls of philox4x32_10_rk on counters (c0, c1, c2, c3a)
+// and (c0, c1, c2, c3b), interleaved round by round so that the two
+// dependency chains overlap (twice the instruction-level parallelism).
+__device__ __forceinline__ void philox4x32_10_rk_x2(uint32_t c0, uint32_t c1, uint32_t c2,
+                                                    uint32_t c3a, uint32_t c3b,
+                                                    const uint32_t *rk, uint32_t a[4],
+                                                    uint32_t b[4]) {
+  uint32_t x0 = c0, x1 = c1, x2 = c2, x3 = c3a;
+  uint32_t y0 = c0, y1 = c1, y2 = c2, y3 = c3b;
+#pragma unroll
+  for (int round = 0; round < 10; ++round) {
+    const uint32_t xl0 = 0xD2511F53u * x0, xh0 = __umulhi(0xD2511F53u, x0);
+    const uint32_t yl0 = 0xD2511F53u * y0, yh0 = __umulhi(0xD2511F53u, y0);
+    const uint32_t xl1 = 0xCD9E8D57u * x2, xh1 = __umulhi(0xCD9E8D57u, x2);
+    const uint32_t yl1 = 0xCD9E8D57u * y2, yh1 = __umulhi(0xCD9E8D57u, y2);
+    const uint32_t k0 = rk[2 * round], k1 = rk[2 * round + 1];
+    x0 = xh1 ^ x1 ^ k0;
+    y0 = yh1 ^ y1 ^ k0;
+    x2 = xh0 ^ x3 ^ k1;
+    y2 = yh0 ^ y3 ^ k1;
+    x1 = xl1;
+    y1 = yl1;
+    x3 = xl0;
+    y3 = yl0;
+  }
+  a[0] = x0; a[1] = x1; a[2] = x2; a[3] = x3;
+  b[0] = y0; b[1] = y1; b[2] = y2; b[3] = y3;
+}
+
 // Uniform on the 24-bit grid ((x >> 8) + 1) * 2^-24, in (0, 1]; exact in
 // float, so host and device agree bit for bit.
 __device__ __forceinline__ float unit24(uint32_t x) {
@@ -134,11 +163,8 @@ __device__ __forceinline__ uint32_t flow_events(uint32_t E, uint32_t I, uint32_t
   const uint32_t r2 = (th.tr_all || th.tr == 0) ? 0u : R;
   uint32_t und = e2 | i2 | r2;
   if (und == 0u) return lt;  // every candidate's threshold is 0 or 1: no draw
-  // the first two calls (8 planes) run unconditionally so that lanes stay in
-  // step; later planes only while some replica is undecided
-  for (int j = 0; j < 16 && (j < 2 || und != 0u); ++j) {
-    uint32_t x[4];
-    philox4x32_10_rk(node, step, word, (uint32_t)j << 4, rk, x);
+  // one random call decides 4 planes for all 32 replicas of the word
+  auto planes = [&](const uint32_t (&x)[4], int j) {
     const int sh = 60 - 4 * j;
     const uint32_t ce = (uint32_t)(th.te >> sh) & 0xFu;
     const uint32_t ci = (uint32_t)(th.ti >> sh) & 0xFu;
@@ -152,6 +178,17 @@ __device__ __forceinline__ uint32_t flow_events(uint32_t E, uint32_t I, uint32_t
       lt |= und & T & ~w;
       und &= ~(T ^ w);
     }
+  };
+  // the first two calls (8 planes) run together, unconditionally; later
+  // planes only while some replica is undecided
+  uint32_t x0[4], x1[4];
+  philox4x32_10_rk_x2(node, step, word, 0u, 1u << 4, rk, x0, x1);
+  planes(x0, 0);
+  planes(x1, 1);
+  for (int j = 2; j < 16 && und != 0u; ++j) {
+    uint32_t x[4];
+    philox4x32_10_rk(node, step, word, (uint32_t)j << 4, rk, x);
+    planes(x, j);
   }
   return lt;
 }
@@ -175,8 +212,7 @@ constexpr uint32_t kTagInfectTail = 12u;
 // The 8 planes of a word's infection uniforms.
 __device__ __forceinline__ void infect_planes(const uint32_t *rk, uint32_t node, uint32_t step,
                                               uint32_t word, uint32_t pl[8]) {
-  philox4x32_10_rk(node, step, word, kTagInfect, rk, pl);
-  philox4x32_10_rk(node, step, word, kTagInfect | 16u, rk, pl + 4);
+  philox4x32_10_rk_x2(node, step, word, kTagInfect, kTagInfect | 16u, rk, pl, pl + 4);
 }
 
 // Top 8 bits of the uniform of replica bit b from its word's planes.

@@ -261,18 +261,21 @@ struct PackedLayout {
 };
 rp_status packed_prepare();  // kernel attributes, once per device
 void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb,
-                 uint32_t *mask, float p0, int32_t k_exact,
+                 uint32_t *mask, uint8_t *flag, float p0, int32_t k_exact,
                  const int32_t *net_first_row, const int32_t *net_rows,
                  int32_t n_nets, const StepConsts &c, cudaStream_t st);
-// One fused kernel per step (step.cu): exposure, infection and flow draws,
-// transitions and event counts; reads mask_in, writes every word of mask_out.
-rp_status step_prepare();  // kernel attributes, once per device
-void packed_step_fused(const PackedLayout &L, const PackedTask *tasks,
-                       const int32_t *row_ptr, const int2 *entries,
-                       const uint32_t *mask_in, uint32_t *mask_out, uint32_t *sa,
-                       uint32_t *sb, unsigned long long *ev_row,
-                       unsigned long long *rs_row, uint32_t step, float scale,
-                       const StepConsts &c, cudaStream_t st);
+// One step: exposure + infection draws (k_infect), then transitions, counts
+// and the next infectious mask (k_flow).
+void packed_infect(const PackedLayout &L, const PackedTask *tasks,
+                   const int32_t *row_ptr, const int2 *entries,
+                   const uint32_t *mask, const uint32_t *sa, const uint32_t *sb,
+                   uint32_t *evs, uint8_t *flag, uint32_t step, float scale,
+                   const StepConsts &c, cudaStream_t st);
+void packed_flow(const PackedLayout &L, const PackedTask *tasks,
+                 const int32_t *row_ptr, uint32_t *mask, uint32_t *sa,
+                 uint32_t *sb, const uint32_t *evs, uint8_t *flag,
+                 unsigned long long *ev_row, unsigned long long *rs_row,
+                 uint32_t step, const StepConsts &c, cudaStream_t st);
 // Batched countdown mode (countdown.cu): per-replica codes into the host's
 // countdown table (next | class << 16 | infectious << 18), 1 or 2 bytes each.
 rp_status cd_prepare();
