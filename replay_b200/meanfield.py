@@ -44,15 +44,20 @@ def _scalar(v, like):
 _LIVE = {}
 
 
+def _f32(t):
+    """A contiguous float32 tensor with t's values (t itself when it is one)."""
+    if t is None or (t.dtype == torch.float32 and t.is_contiguous()):
+        return t
+    return t.to(torch.float32).contiguous()
+
+
 @torch.library.custom_op("replay_b200::meanfield", mutates_args=())
 def meanfield_op(handle: int, x0: torch.Tensor, beta: torch.Tensor, sus: Optional[torch.Tensor],
                  p_ei: torch.Tensor, p_ir: torch.Tensor, p_rs: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
     """Expected-value replay of MeanField `handle` (rp_meanfield_forward):
     returns (incidence (T,), x_T (4, N)) in float32 on the graph's GPU."""
     mf = _LIVE[handle]
-    x0c = x0.detach().to(torch.float32).contiguous()
-    susc = sus.detach().to(torch.float32).contiguous() if sus is not None else None
-    return mf._forward(x0c, susc, [float(v) for v in (beta, p_ei, p_ir, p_rs)])
+    return mf._forward(_f32(x0), _f32(sus), [float(v) for v in (beta, p_ei, p_ir, p_rs)])
 
 
 @meanfield_op.register_fake
@@ -66,8 +71,7 @@ def _setup_context(ctx, inputs, output):
     mf = _LIVE[handle]
     ctx.handle = handle
     ctx.generation = mf._generation
-    ctx.inputs = (x0.detach().to(torch.float32).contiguous(),
-                  sus.detach().to(torch.float32).contiguous() if sus is not None else None,
+    ctx.inputs = (_f32(x0.detach()), _f32(sus.detach()) if sus is not None else None,
                   [float(v) for v in (beta, p_ei, p_ir, p_rs)])
     ctx.has_sus = sus is not None
     ctx.rate_dtypes = [v.dtype for v in (beta, p_ei, p_ir, p_rs)]
@@ -79,8 +83,7 @@ def _backward(ctx, g_inc, g_xT):
     if mf._generation != ctx.generation:  # another forward ran since: restore its checkpoints
         mf._forward(*ctx.inputs)
     dev = mf.device
-    g_inc = g_inc.to(torch.float32).contiguous() if g_inc is not None else None
-    g_xT = g_xT.to(torch.float32).contiguous() if g_xT is not None else None
+    g_inc, g_xT = _f32(g_inc), _f32(g_xT)
     gx0 = torch.empty((4, mf.N), dtype=torch.float32, device=dev)
     gsus = torch.empty(mf.N, dtype=torch.float32, device=dev) if ctx.has_sus else None
     grates = torch.empty(4, dtype=torch.float64, device=dev)
