@@ -229,9 +229,11 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
   Q.off[lane] = warp_excl_scan(__popc(Cw), lane, ctotal);
   __syncwarp();
   // ---- phase 3: exact test of 32 candidates at a time ----
-  // The batch's (candidate, CSR pair) products are spread over the lanes:
-  // every pair is one independent mask-word load (a long row is shared by
-  // all 32 lanes), and the exposures sum in shared memory (exact int64).
+  // When every candidate's row is short, each lane sums its own row.
+  // Otherwise the batch's (candidate, CSR pair) products are spread over the
+  // lanes: every pair is one independent mask-word load (a long row is
+  // shared by all 32 lanes), and the exposures sum in shared memory (exact
+  // int64).
   const int nk = Q.nk;
   const int total = nk + ctotal;
   int base = 0;
@@ -257,6 +259,24 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
       beg = s_rp[orl];
       npairs = s_rp[orl + 1] - beg;
     }
+    long long e = 0;
+    if (__reduce_max_sync(kFull, (unsigned)npairs) <= 32u) {
+      // short rows: each lane sums its own row (loads two pairs ahead)
+      int32_t k = beg;
+      const int32_t kend = beg + npairs;
+      for (; k + 1 < kend; k += 2) {
+        const int2 q0 = staged ? s_ent[k - e0] : __ldg(ent + k);
+        const int2 q1 = staged ? s_ent[k + 1 - e0] : __ldg(ent + k + 1);
+        const uint32_t m0 = mask_w[(int64_t)q0.x * L.words + word];
+        const uint32_t m1 = mask_w[(int64_t)q1.x * L.words + word];
+        e += ((m0 >> b) & 1u) ? q0.y : 0;
+        e += ((m1 >> b) & 1u) ? q1.y : 0;
+      }
+      if (k < kend) {
+        const int2 q0 = staged ? s_ent[k - e0] : __ldg(ent + k);
+        e += ((mask_w[(int64_t)q0.x * L.words + word] >> b) & 1u) ? q0.y : 0;
+      }
+    } else {
     int ptotal;
     const int poff = warp_excl_scan(npairs, lane, ptotal);
     __syncwarp();
@@ -293,9 +313,10 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
                     (unsigned long long)(long long)pw[h]);
     }
     __syncwarp();
+    e = Q.esum[lane];
+    }
     if (p >= total) continue;
     const int orow = T.row_begin + orl;
-    const long long e = Q.esum[lane];
     const float br = c.beta_r ? s_beta[(word - 4 * cbase) * 32 + b] : c.beta;
     const float bs = c.sus ? __fmul_rn(br, c.sus[orow]) : br;
     float ef = __ll2float_rn(e);
