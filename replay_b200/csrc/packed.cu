@@ -491,89 +491,114 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       const int nitems = (r1 - r0) * ncols;
       // warp-uniform; one pass past the items decides what is left queued
-      // (the staged pairs change with the next chunk)
-      for (int it0 = warp * 32;; it0 += kWarps * 32) {
+      // (the staged pairs change with the next chunk).  Two items per lane
+      // per pass: their plane words and their neighbours' mask words are
+      // all in flight together.
+      for (int it0 = warp * 64;; it0 += kWarps * 64) {
         const bool flushing = it0 >= nitems;
         // ---- phase 1: gather, per lane ----
-        const int it = it0 + lane;
-        const bool ok = it < nitems;
-        const int rl = ok ? (int)dv.div((uint32_t)it) : 0;
-        const int cc = ok ? it - rl * ncols : 0;
-        const int rloc = r0 + rl;
-        const int col = cbase + cc;
-        const int row = T.row_begin + rloc;
-        const int32_t beg = s_rp[rloc], end = s_rp[rloc + 1];
-        const int n = ok ? end - beg : 0;
-        uint32_t X[4] = {0, 0, 0, 0};
-        float efmax = 0.0f;
-        if (n > 0) {
-          const int64_t idx = (int64_t)row * L.q4 + col;
-          const uint4 a4 = sa[idx], b4 = sb[idx];
-          const int2 *er = s_ent + (beg - e0);
-          uint4 inf = make_uint4(0, 0, 0, 0);
-          long long emax = 0;
-          int k = 0;
-          if (long_row) {  // gathered by the whole CTA above
-            inf = s_lor[cc];
-            emax = s_lemax;
-            k = n;
+        int rlocs[2], cols[2], nn[2];
+        const int2 *er[2];
+        uint4 a4[2], b4[2], inf[2];
+        long long emax[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int it = it0 + 32 * h + lane;
+          const bool ok = it < nitems;
+          const int rl = ok ? (int)dv.div((uint32_t)it) : 0;
+          const int cc = ok ? it - rl * ncols : 0;
+          rlocs[h] = r0 + rl;
+          cols[h] = cbase + cc;
+          const int32_t beg = s_rp[rlocs[h]];
+          nn[h] = ok ? s_rp[rlocs[h] + 1] - beg : 0;
+          er[h] = s_ent + (beg - e0);
+          inf[h] = make_uint4(0, 0, 0, 0);
+          emax[h] = 0;
+          a4[h] = b4[h] = make_uint4(0, 0, 0, 0);
+          if (nn[h] > 0) {
+            const int64_t idx = (int64_t)(T.row_begin + rlocs[h]) * L.q4 + cols[h];
+            a4[h] = sa[idx];
+            b4[h] = sb[idx];
           }
-          for (; k + 4 <= n; k += 4) {
-            const int2 q0 = er[k], q1 = er[k + 1], q2 = er[k + 2], q3 = er[k + 3];
-            const uint4 m0 = mask_in[(int64_t)q0.x * L.q4 + col];
-            const uint4 m1 = mask_in[(int64_t)q1.x * L.q4 + col];
-            const uint4 m2 = mask_in[(int64_t)q2.x * L.q4 + col];
-            const uint4 m3 = mask_in[(int64_t)q3.x * L.q4 + col];
-            or4(inf, m0);
-            or4(inf, m1);
-            or4(inf, m2);
-            or4(inf, m3);
-            emax += (long long)q0.y + q1.y + q2.y + q3.y;
+          if (long_row && nn[h] > 0) {  // gathered by the whole CTA above
+            inf[h] = s_lor[cc];
+            emax[h] = s_lemax;
+            nn[h] = -nn[h];  // gathered: skip the pairs below
           }
-          for (; k < n; ++k) {
-            const int2 q0 = er[k];
-            or4(inf, mask_in[(int64_t)q0.x * L.q4 + col]);
-            emax += q0.y;
+        }
+        // two pairs of each item per round trip (predicated tails)
+        const int nmax = max(max(nn[0], nn[1]), 0);
+        for (int k = 0; k < nmax; k += 2) {
+          int2 q[2][2];
+          uint4 m[2][2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+              q[h][j] = k + j < nn[h] ? er[h][k + j] : make_int2(0, 0);
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+              m[h][j] = k + j < nn[h] ? mask_in[(int64_t)q[h][j].x * L.q4 + cols[h]]
+                                      : make_uint4(0, 0, 0, 0);
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              or4(inf[h], m[h][j]);
+              emax[h] += q[h][j].y;
+            }
+        }
+        // ---- queue the exposed words of each item, deciding full rounds
+        // after each (and, past the items, the remainder and the carried
+        // candidates: the staged pairs change with the chunk) ----
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+          const uint4 infh = h ? inf[1] : inf[0], ah = h ? a4[1] : a4[0], bh = h ? b4[1] : b4[0];
+          const int colh = h ? cols[1] : cols[0], rloch = h ? rlocs[1] : rlocs[0];
+          const long long emaxh = h ? emax[1] : emax[0];
+          uint32_t X[4] = {0, 0, 0, 0};
+          float efmax = 0.0f;
+          if ((h ? nn[1] : nn[0]) != 0) {
+#pragma unroll
+            for (int w = 0; w < 4; ++w)
+              X[w] = get4(infh, w) & ~get4(ah, w) & ~get4(bh, w) & word_mask(L, 4 * colh + w);
+            efmax = __ll2float_rn(emaxh);
+            if (scale != 1.0f) efmax = __fmul_rn(efmax, scale);
           }
 #pragma unroll
-          for (int w = 0; w < 4; ++w)
-            X[w] = get4(inf, w) & ~get4(a4, w) & ~get4(b4, w) & word_mask(L, 4 * col + w);
-          efmax = __ll2float_rn(emax);
-          if (scale != 1.0f) efmax = __fmul_rn(efmax, scale);
-        }
-        // ---- queue the exposed words ----
-#pragma unroll
-        for (int w = 0; w < 4; ++w) {
-          const unsigned qm = __ballot_sync(kFull, X[w] != 0u);
-          if (!qm) continue;
-          const int base = Q.n;
-          if (X[w]) {
-            const int pos = base + __popc(qm & ((1u << lane) - 1u));
-            Q.rloc[pos] = rloc;
-            Q.word[pos] = 4 * col + w;
-            Q.X[pos] = X[w];
-            Q.efmax[pos] = efmax;
+          for (int w = 0; w < 4; ++w) {
+            const unsigned qm = __ballot_sync(kFull, X[w] != 0u);
+            if (!qm) continue;
+            const int base = Q.n;
+            if (X[w]) {
+              const int pos = base + __popc(qm & ((1u << lane) - 1u));
+              Q.rloc[pos] = rloch;
+              Q.word[pos] = 4 * colh + w;
+              Q.X[pos] = X[w];
+              Q.efmax[pos] = efmax;
+            }
+            __syncwarp();
+            if (lane == 0) Q.n = base + __popc(qm);
+            __syncwarp();
           }
-          __syncwarp();
-          if (lane == 0) Q.n = base + __popc(qm);
-          __syncwarp();
-        }
-        // ---- decide full rounds (and, past the items, the remainder and
-        // the carried candidates: the staged pairs change with the chunk) ----
-        while (Q.n >= 32 || (flushing && (Q.n > 0 || Q.nk > 0))) {
-          const int take = Q.n < 32 ? Q.n : 32;
-          infect_round(Q, take, flushing && take == Q.n, lane, L, T, cbase, s_rp, s_ent, ent,
-                       staged, e0, s_beta, s_bw, mask_w, evs_w, flag32, step, scale, c);
-          const int rest = Q.n - take;
-          for (int i = lane; i < rest; i += 32) {
-            Q.rloc[i] = Q.rloc[take + i];
-            Q.word[i] = Q.word[take + i];
-            Q.X[i] = Q.X[take + i];
-            Q.efmax[i] = Q.efmax[take + i];
+          const bool drain = flushing && h == 1;
+          while (Q.n >= 32 || (drain && (Q.n > 0 || Q.nk > 0))) {
+            const int take = Q.n < 32 ? Q.n : 32;
+            infect_round(Q, take, drain && take == Q.n, lane, L, T, cbase, s_rp, s_ent, ent,
+                         staged, e0, s_beta, s_bw, mask_w, evs_w, flag32, step, scale, c);
+            const int rest = Q.n - take;
+            for (int i = lane; i < rest; i += 32) {
+              Q.rloc[i] = Q.rloc[take + i];
+              Q.word[i] = Q.word[take + i];
+              Q.X[i] = Q.X[take + i];
+              Q.efmax[i] = Q.efmax[take + i];
+            }
+            __syncwarp();
+            if (lane == 0) Q.n = rest;
+            __syncwarp();
           }
-          __syncwarp();
-          if (lane == 0) Q.n = rest;
-          __syncwarp();
         }
         if (flushing) break;
       }
@@ -596,6 +621,17 @@ __device__ __forceinline__ void count_bits(unsigned long long *s_ev, int wl, uin
 }
 
 // Applies one word's moves; returns the new planes and counts the events.
+// Per-replica event counters of a task slice in shared memory, two 32-bit
+// words per replica (32-bit shared atomics): c0 = S->E | ->I << 16,
+// c1 = I-> | R->S << 16 (a task has at most 1024 rows).
+__device__ __forceinline__ void count_bits32(uint32_t *s_c, int wl, uint32_t t, uint32_t inc) {
+  while (t) {
+    const int r = __ffs(t) - 1;
+    atomicAdd(&s_c[wl * 32 + r], inc);
+    t &= t - 1;
+  }
+}
+
 __device__ __forceinline__ void apply_word(uint32_t A, uint32_t B, uint32_t evS, uint32_t f,
                                            bool waning, const StepConsts &c,
                                            unsigned long long *s_ev, int wl, uint32_t &na,
@@ -618,10 +654,11 @@ __device__ __forceinline__ void apply_word(uint32_t A, uint32_t B, uint32_t evS,
   na = xa;
   nb = xb;
   if (evS | evE | evI | evR) {
-    count_bits(s_ev, wl, c.has_exposed ? evS : 0u, 1ull);
-    count_bits(s_ev, wl, evE | (c.has_exposed ? 0u : evS), 1ull << 16);
-    count_bits(s_ev, wl, evI, 1ull << 32);
-    count_bits(s_ev, wl, evR, 1ull << 48);
+    uint32_t *c0 = reinterpret_cast<uint32_t *>(s_ev), *c1 = c0 + 128 * 32;
+    count_bits32(c0, wl, c.has_exposed ? evS : 0u, 1u);
+    count_bits32(c0, wl, evE | (c.has_exposed ? 0u : evS), 1u << 16);
+    count_bits32(c1, wl, evI, 1u);
+    count_bits32(c1, wl, evR, 1u << 16);
   }
 }
 
@@ -802,7 +839,8 @@ __global__ void __launch_bounds__(kThreads, 3)
     }
     __syncthreads();
     for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x) {
-      const unsigned long long v = s_ev[j];
+      const uint32_t *c0 = reinterpret_cast<const uint32_t *>(s_ev), *c1 = c0 + 128 * 32;
+      const unsigned long long v = (unsigned long long)c0[j] | ((unsigned long long)c1[j] << 32);
       if (!v) continue;
       const int rep = cbase * 128 + j;
       if (rep >= L.m) continue;
