@@ -103,6 +103,13 @@ __device__ __forceinline__ int find_owner(const int32_t *off, int p) {
 
 constexpr int kMaxTaskRows = 1024;  // rows of one task (host-side limit)
 
+// Per-item hint byte (item = node x 4-word column): bit 0 an infection event
+// of this step (k_infect), bit 1 replicas that may move (E, I, waning R),
+// bit 2 replicas that may be susceptible.  k_flow rewrites bits 1-2 from the
+// start-of-step planes of every item it reads, as a superset of the next
+// step's state; items without events and without bit 1 are not read.
+constexpr uint8_t kFlagEvent = 1, kFlagActive = 2, kFlagSusceptible = 4;
+
 constexpr int kEntCap = 768;        // staged CSR pairs per chunk
 constexpr int kEntBuf = kEntCap + 4; // a staging buffer (the copy may start one pair early)
 constexpr int kPiece = kEntBuf / 2 - 2;  // pairs per piece of a long row (a half buffer)
@@ -376,6 +383,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t *mask_w = reinterpret_cast<const uint32_t *>(mask_in);
   uint32_t *evs_w = reinterpret_cast<uint32_t *>(evs);
+  const uint8_t *flag8 = reinterpret_cast<const uint8_t *>(flag32);
   if (lane == 0) {
     Q.n = 0;
     Q.nk = 0;
@@ -515,11 +523,10 @@ __global__ void __launch_bounds__(kThreads, 3)
           inf[h] = make_uint4(0, 0, 0, 0);
           emax[h] = 0;
           a4[h] = b4[h] = make_uint4(0, 0, 0, 0);
-          if (nn[h] > 0) {
-            const int64_t idx = (int64_t)(T.row_begin + rlocs[h]) * L.q4 + cols[h];
-            a4[h] = sa[idx];
-            b4[h] = sb[idx];
-          }
+          // an item without susceptible replicas cannot be infected
+          if (nn[h] > 0 &&
+              !(flag8[(int64_t)(T.row_begin + rlocs[h]) * L.q4 + cols[h]] & kFlagSusceptible))
+            nn[h] = 0;
           if (long_row && nn[h] > 0) {  // gathered by the whole CTA above
             inf[h] = s_lor[cc];
             emax[h] = s_lemax;
@@ -550,6 +557,14 @@ __global__ void __launch_bounds__(kThreads, 3)
               emax[h] += q[h][j].y;
             }
         }
+        // the planes only of items with an infectious neighbour
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (nn[h] != 0 && (inf[h].x | inf[h].y | inf[h].z | inf[h].w)) {
+            const int64_t idx = (int64_t)(T.row_begin + rlocs[h]) * L.q4 + cols[h];
+            a4[h] = sa[idx];
+            b4[h] = sb[idx];
+          }
         // ---- queue the exposed words of each item, deciding full rounds
         // after each (and, past the items, the remainder and the carried
         // candidates: the staged pairs change with the chunk) ----
@@ -746,10 +761,15 @@ __global__ void __launch_bounds__(kThreads, 3)
         rl[h] = in[h] ? (int)dv.div((uint32_t)itv) : 0;
         cl[h] = in[h] ? itv - rl[h] * ncols : 0;
         const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
+        st[h] = in[h] ? flag[idx] : 0;
+      }
+      // the planes of items that may move (an infection event, or replicas
+      // that may be E, I or waning R): the others are skipped unread
+#pragma unroll
+      for (int h = 0; h < kFlowIPL; ++h) {
+        const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
         a4[h] = b4[h] = make_uint4(0, 0, 0, 0);
-        st[h] = 0;
-        if (in[h]) {
-          st[h] = flag[idx];
+        if (st[h] & (kFlagEvent | kFlagActive)) {
           a4[h] = sa[idx];
           b4[h] = sb[idx];
         }
@@ -769,17 +789,32 @@ __global__ void __launch_bounds__(kThreads, 3)
           if (valid && (waning ? (A | B) : (A ^ B)) != 0u) cm[h] |= 1u << w;
         }
         cnt += __popc(cm[h]);
-        busy |= st[h] != 0 || cm[h] != 0;
+        busy |= (st[h] & kFlagEvent) != 0 || cm[h] != 0;
+        // next step's hint byte, from this step's planes and events: a
+        // superset of the items that can move (E, I, waning R, or newly
+        // infected) and of those with susceptible replicas
+        if (st[h] & (kFlagEvent | kFlagActive)) {
+          bool act = (st[h] & kFlagEvent) != 0, sus = false;
+#pragma unroll
+          for (int w = 0; w < 4; ++w) {
+            const uint32_t A = get4(a4[h], w), B = get4(b4[h], w);
+            const uint32_t vm = word_mask(L, 4 * (cbase + cl[h]) + w);
+            act |= (((A ^ B) | (waning ? (A & B) : 0u)) & vm) != 0u;
+            // S now, or back to S this step (waning R, or I -> S)
+            sus |= ((~A & ~B) | (waning ? (A & B) : 0u) | (c.ir_to_s ? (A & ~B) : 0u)) & vm;
+          }
+          const uint8_t nb = (uint8_t)((act ? kFlagActive : 0) | (sus ? kFlagSusceptible : 0));
+          if (nb != st[h]) flag[(int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h]] = nb;
+        }
       }
       if (!flushing && !__any_sync(kFull, busy)) continue;
       // infection events: words without flow candidates are applied here;
       // the queued words' events are read (and cleared) by their round
 #pragma unroll
       for (int h = 0; h < kFlowIPL; ++h) {
-        if (!st[h]) continue;
+        if (!(st[h] & kFlagEvent)) continue;
         const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
         const uint4 e4 = evs[idx];
-        flag[idx] = 0;
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
           const uint32_t ev = get4(e4, w);
@@ -948,6 +983,27 @@ __global__ void k_mask_from_planes(int64_t total, const uint32_t *__restrict__ s
     mask[i] = sa[i] & ~sb[i];
 }
 
+// Hint bytes of every item from the initial planes (kFlagActive: E, I or
+// waning R replicas; kFlagSusceptible: S replicas).
+__global__ void k_flag_from_planes(PackedLayout L, const uint4 *__restrict__ sa,
+                                   const uint4 *__restrict__ sb, uint8_t *__restrict__ flag,
+                                   bool waning) {
+  const int64_t total = (int64_t)L.n_nodes * L.q4;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint4 a4 = sa[i], b4 = sb[i];
+    const int col = (int)(i % L.q4);
+    bool act = false, sus = false;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const uint32_t A = get4(a4, w), B = get4(b4, w), vm = word_mask(L, 4 * col + w);
+      act |= (((A ^ B) | (waning ? (A & B) : 0u)) & vm) != 0u;
+      sus |= ((~A & ~B) & vm) != 0u;
+    }
+    flag[i] = (uint8_t)((act ? kFlagActive : 0) | (sus ? kFlagSusceptible : 0));
+  }
+}
+
 // counts[t][net][r][4] from the initial counts and the per-step events.
 __global__ void k_finalize(const unsigned long long *__restrict__ init,
                            const unsigned long long *__restrict__ ev,
@@ -1042,6 +1098,9 @@ void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb, uint32_t *ma
     k_mask_from_planes<<<1184, 256, 0, st>>>(total, sa, sb, mask);
   }
   cudaMemsetAsync(flag, 0, ((size_t)L.n_nodes * L.q4 + 3) / 4 * 4, st);
+  k_flag_from_planes<<<1184, 256, 0, st>>>(L, reinterpret_cast<const uint4 *>(sa),
+                                           reinterpret_cast<const uint4 *>(sb), flag,
+                                           c.th.tr_all || c.th.tr != 0);
 }
 
 void packed_step(const PackedLayout &L, const PackedTask *tasks, const int32_t *row_ptr,
