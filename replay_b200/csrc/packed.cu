@@ -52,6 +52,10 @@ __device__ __forceinline__ uint32_t get4(const uint4 &v, int w) {
   return w == 0 ? v.x : (w == 1 ? v.y : (w == 2 ? v.z : v.w));
 }
 
+__device__ __forceinline__ void set4(uint4 &v, int w, uint32_t x) {
+  if (w == 0) v.x = x; else if (w == 1) v.y = x; else if (w == 2) v.z = x; else v.w = x;
+}
+
 __device__ __forceinline__ void or4(uint4 &a, const uint4 b) {
   a.x |= b.x;
   a.y |= b.y;
@@ -105,9 +109,10 @@ constexpr int kMaxTaskRows = 1024;  // rows of one task (host-side limit)
 
 // Per-item hint byte (item = node x 4-word column): bit 0 an infection event
 // of this step (k_infect), bit 1 replicas that may move (E, I, waning R),
-// bit 2 replicas that may be susceptible.  k_flow rewrites bits 1-2 from the
-// start-of-step planes of every item it reads, as a superset of the next
-// step's state; items without events and without bit 1 are not read.
+// bit 2 replicas that may be susceptible.  k_flow rewrites bits 1-2 of every
+// item from its start-of-step planes and events, as a superset of the next
+// step's state; k_infect skips the neighbours of items without bit 2 where
+// rows are long enough for the extra load to pay.
 constexpr uint8_t kFlagEvent = 1, kFlagActive = 2, kFlagSusceptible = 4;
 
 constexpr int kEntCap = 768;        // staged CSR pairs per chunk
@@ -209,7 +214,7 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
                                              const PackedLayout &L, const PackedTask &T,
                                              int cbase, const int32_t *s_rp, const int2 *s_ent,
                                              const int2 *__restrict__ ent, bool staged,
-                                             int32_t e0, const float *s_beta, const float *s_bw,
+                                             int32_t e0, const float *s_bw,
                                              const uint32_t *mask_w, uint32_t *evs_w,
                                              uint32_t *flag32, uint32_t step, float scale,
                                              const StepConsts &c) {
@@ -324,7 +329,7 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
     }
     if (p >= total) continue;
     const int orow = T.row_begin + orl;
-    const float br = c.beta_r ? s_beta[(word - 4 * cbase) * 32 + b] : c.beta;
+    const float br = c.beta_r ? __ldg(c.beta_r + word * 32 + b) : c.beta;
     const float bs = c.sus ? __fmul_rn(br, c.sus[orow]) : br;
     float ef = __ll2float_rn(e);
     if (scale != 1.0f) ef = __fmul_rn(ef, scale);
@@ -377,7 +382,8 @@ __global__ void __launch_bounds__(kThreads, 3)
   extern __shared__ __align__(16) unsigned char s_dyn[];
   int2 *const s_buf0 = reinterpret_cast<int2 *>(s_dyn);  // two staging buffers of kEntBuf pairs
   auto bufp = [&](int b) { return s_buf0 + b * kEntBuf; };
-  float *s_beta = reinterpret_cast<float *>(s_dyn + 2 * kEntBuf * sizeof(int2));
+  // a long row's per-replica exposures (int32, ncols x 128 replicas)
+  int32_t *s_acc = reinterpret_cast<int32_t *>(s_dyn + 2 * kEntBuf * sizeof(int2));
   InfectQueue &Q = reinterpret_cast<InfectQueue *>(
       s_dyn + 2 * kEntBuf * sizeof(int2) + 128 * 32 * sizeof(float))[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -407,16 +413,15 @@ __global__ void __launch_bounds__(kThreads, 3)
     const Div dv((uint32_t)ncols);
     const int nrows = T.row_end - T.row_begin;
     for (int i = threadIdx.x; i <= nrows; i += blockDim.x) s_rp[i] = row_ptr[T.row_begin + i];
-    if (c.beta_r) {
-      for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x)
-        s_beta[j] = cbase * 128 + j < L.m ? c.beta_r[cbase * 128 + j] : 0.0f;
-      __syncthreads();
+    if (c.beta_r)
       for (int wl = threadIdx.x; wl < ncols * 4; wl += blockDim.x) {
         float mx = 0.0f;
-        for (int r = 0; r < 32; ++r) mx = fmaxf(mx, fabsf(s_beta[wl * 32 + r]));
+        for (int r = 0; r < 32; ++r) {
+          const int rep = cbase * 128 + wl * 32 + r;
+          if (rep < L.m) mx = fmaxf(mx, fabsf(__ldg(c.beta_r + rep)));
+        }
         s_bw[wl] = mx;
       }
-    }
     __syncthreads();
     // chunk of rows [r0, end) whose CSR pairs fit a staging buffer (>= 1 row)
     auto chunk_end = [&](int r0) {
@@ -442,11 +447,32 @@ __global__ void __launch_bounds__(kThreads, 3)
       const bool staged = e1 - e0 <= kEntCap;
       if (staged && e1 > e0) wait_bar(buf, cph, buf);
       const int2 *s_ent = bufp(buf) + pair_shift(ent, e0);
-      const bool long_row = !staged;  // one row with more pairs than a buffer
+      // one row with more pairs than a buffer; streamed only when one of
+      // its items may hold susceptible replicas
+      const bool long_row =
+          !staged && __syncthreads_or(threadIdx.x < ncols &&
+                                      (flag8[(int64_t)(T.row_begin + r0) * L.q4 + cbase +
+                                             threadIdx.x] & kFlagSusceptible));
+      const bool skip_row = !staged && !long_row;
+      const bool use_hint = e1 - e0 >= 8 * (r1 - r0);  // at least 8 pairs per row
+      bool dense_done = false;
       if (long_row) {
-        // its pairs stream through the two halves of this chunk's buffer, one
-        // piece ahead; every warp ORs the neighbours' mask words of its share
-        // of a piece (lane = column) and the shares combine in shared memory
+        // A hub of the window graph.  Its pairs stream through the two halves
+        // of this chunk's buffer, one piece ahead; every warp takes a share
+        // of each piece (lane = column: a pair costs one 512-byte line of mask
+        // words) and, for the susceptible replicas of the row, adds the
+        // pair's contact-seconds to each infectious neighbour replica's exact
+        // exposure in shared memory.  Every exposed replica is then decided
+        // from its exposure directly (no bound test, no per-candidate scan).
+        const int64_t row = T.row_begin + r0;
+        uint4 S4 = make_uint4(0, 0, 0, 0);
+        if (lane < ncols) {
+          const uint4 a4 = sa[row * L.q4 + cbase + lane], b4 = sb[row * L.q4 + cbase + lane];
+#pragma unroll
+          for (int w = 0; w < 4; ++w)
+            set4(S4, w, ~get4(a4, w) & ~get4(b4, w) & word_mask(L, 4 * (cbase + lane) + w));
+        }
+        for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x) s_acc[j] = 0;
         int2 *const half0 = bufp(buf);
         auto half = [&](int h) { return half0 + h * (kEntBuf / 2); };
         if (threadIdx.x < 32) s_lor[threadIdx.x] = make_uint4(0, 0, 0, 0);
@@ -454,8 +480,17 @@ __global__ void __launch_bounds__(kThreads, 3)
           s_lemax = 0;
           stage_pairs(half(0), ent, e0, min(e0 + kPiece, e1), &s_bar[2]);
         }
+        __syncthreads();
         uint4 linf = make_uint4(0, 0, 0, 0);
         long long lemax = 0;
+        auto add_pair = [&](int2 q, uint4 m) {
+          m = make_uint4(m.x & S4.x, m.y & S4.y, m.z & S4.z, m.w & S4.w);
+          or4(linf, m);
+#pragma unroll
+          for (int w = 0; w < 4; ++w)
+            for (uint32_t t = get4(m, w); t; t &= t - 1)
+              atomicAdd(&s_acc[(lane * 4 + w) * 32 + __ffs(t) - 1], q.y);
+        };
         const int npieces = (e1 - e0 + kPiece - 1) / kPiece;
         for (int pk = 0; pk < npieces; ++pk) {
           const int hb = pk & 1;
@@ -465,25 +500,20 @@ __global__ void __launch_bounds__(kThreads, 3)
           wait_bar(2 + hb, pph, hb);
           const int2 *pc = half(hb) + pair_shift(ent, p0);
           int32_t k = p0 + warp;
-          for (; k + 3 * kWarps < p1; k += 4 * kWarps) {
-            const int2 q0 = pc[k - p0], q1 = pc[k - p0 + kWarps], q2 = pc[k - p0 + 2 * kWarps],
-                       q3 = pc[k - p0 + 3 * kWarps];
+          for (; k + kWarps < p1; k += 2 * kWarps) {
+            const int2 q0 = pc[k - p0], q1 = pc[k - p0 + kWarps];
+            lemax += (long long)q0.y + q1.y;
             if (lane < ncols) {
               const uint4 m0 = mask_in[(int64_t)q0.x * L.q4 + cbase + lane];
               const uint4 m1 = mask_in[(int64_t)q1.x * L.q4 + cbase + lane];
-              const uint4 m2 = mask_in[(int64_t)q2.x * L.q4 + cbase + lane];
-              const uint4 m3 = mask_in[(int64_t)q3.x * L.q4 + cbase + lane];
-              or4(linf, m0);
-              or4(linf, m1);
-              or4(linf, m2);
-              or4(linf, m3);
+              add_pair(q0, m0);
+              add_pair(q1, m1);
             }
-            lemax += (long long)q0.y + q1.y + q2.y + q3.y;
           }
           for (; k < p1; k += kWarps) {
             const int2 q0 = pc[k - p0];
-            if (lane < ncols) or4(linf, mask_in[(int64_t)q0.x * L.q4 + cbase + lane]);
             lemax += q0.y;
+            if (lane < ncols) add_pair(q0, mask_in[(int64_t)q0.x * L.q4 + cbase + lane]);
           }
           __syncthreads();  // the half is free to restage
         }
@@ -496,124 +526,130 @@ __global__ void __launch_bounds__(kThreads, 3)
         if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long *>(&s_lemax),
                                  (unsigned long long)lemax);
         __syncthreads();
+        // int32 sums are exact while the row's total fits; otherwise its
+        // items take the per-candidate exact test below
+        dense_done = s_lemax <= 0x7FFFFFFFll;
+        if (dense_done) {
+          const uint32_t *lor = reinterpret_cast<const uint32_t *>(s_lor);
+          const float bs_row = c.sus ? __ldg(c.sus + row) : 1.0f;
+          for (int wl = threadIdx.x; wl < ncols * 4; wl += blockDim.x) {
+            const uint32_t X = lor[wl];  // exposed replicas of the word
+            if (!X) continue;
+            const int word = 4 * cbase + wl;
+            uint32_t pl[8];
+            infect_planes(c.rk, (uint32_t)row, step, (uint32_t)word + (c.roff >> 5), pl);
+            uint32_t ev = 0;
+            for (uint32_t t = X; t; t &= t - 1) {
+              const int b = __ffs(t) - 1;
+              const float br = c.beta_r ? __ldg(c.beta_r + word * 32 + b) : c.beta;
+              const float bs = c.sus ? __fmul_rn(br, bs_row) : br;
+              float ef = __int2float_rn(s_acc[wl * 32 + b]);
+              if (scale != 1.0f) ef = __fmul_rn(ef, scale);
+              const float xx = __fmul_rn(bs, ef);
+              if (!(xx > 0.0f)) continue;
+              const uint32_t u8 = top8_of(pl, (uint32_t)b);
+              if (xx < 1.0f && u8 > (uint32_t)(fixed64(xx) >> 56)) continue;
+              const uint32_t gword = (uint32_t)word + (c.roff >> 5);
+              if (infect_event(one_minus_exp_neg(xx), u8, c.rk, (uint32_t)row, step,
+                               gword * 32u + (uint32_t)b))
+                ev |= 1u << b;
+            }
+            if (ev) {
+              atomicOr(&evs_w[row * L.words + word], ev);
+              const int64_t idx = row * L.q4 + (word >> 2);
+              atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
+            }
+          }
+        }
+        __syncthreads();
       }
-      const int nitems = (r1 - r0) * ncols;
+      const int nitems = skip_row || dense_done ? 0 : (r1 - r0) * ncols;
       // warp-uniform; one pass past the items decides what is left queued
-      // (the staged pairs change with the next chunk).  Two items per lane
-      // per pass: their plane words and their neighbours' mask words are
-      // all in flight together.
-      for (int it0 = warp * 64;; it0 += kWarps * 64) {
+      // (the staged pairs change with the next chunk)
+      for (int it0 = warp * 32;; it0 += kWarps * 32) {
         const bool flushing = it0 >= nitems;
         // ---- phase 1: gather, per lane ----
-        int rlocs[2], cols[2], nn[2];
-        const int2 *er[2];
-        uint4 a4[2], b4[2], inf[2];
-        long long emax[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int it = it0 + 32 * h + lane;
-          const bool ok = it < nitems;
-          const int rl = ok ? (int)dv.div((uint32_t)it) : 0;
-          const int cc = ok ? it - rl * ncols : 0;
-          rlocs[h] = r0 + rl;
-          cols[h] = cbase + cc;
-          const int32_t beg = s_rp[rlocs[h]];
-          nn[h] = ok ? s_rp[rlocs[h] + 1] - beg : 0;
-          er[h] = s_ent + (beg - e0);
-          inf[h] = make_uint4(0, 0, 0, 0);
-          emax[h] = 0;
-          a4[h] = b4[h] = make_uint4(0, 0, 0, 0);
-          // an item without susceptible replicas cannot be infected
-          if (nn[h] > 0 &&
-              !(flag8[(int64_t)(T.row_begin + rlocs[h]) * L.q4 + cols[h]] & kFlagSusceptible))
-            nn[h] = 0;
-          if (long_row && nn[h] > 0) {  // gathered by the whole CTA above
-            inf[h] = s_lor[cc];
-            emax[h] = s_lemax;
-            nn[h] = -nn[h];  // gathered: skip the pairs below
+        const int it = it0 + lane;
+        const bool ok = it < nitems;
+        const int rl = ok ? (int)dv.div((uint32_t)it) : 0;
+        const int cc = ok ? it - rl * ncols : 0;
+        const int rloc = r0 + rl;
+        const int col = cbase + cc;
+        const int row = T.row_begin + rloc;
+        const int32_t beg = s_rp[rloc], end = s_rp[rloc + 1];
+        const int64_t idx = (int64_t)row * L.q4 + col;
+        // an item without susceptible replicas cannot be infected: on
+        // pair-heavy chunks the hint byte saves the item's whole gather
+        const int n = ok && (!use_hint || (flag8[idx] & kFlagSusceptible)) ? end - beg : 0;
+        uint32_t X[4] = {0, 0, 0, 0};
+        float efmax = 0.0f;
+        if (n > 0) {
+          const uint4 a4 = sa[idx], b4 = sb[idx];
+          const int2 *er = s_ent + (beg - e0);
+          uint4 inf = make_uint4(0, 0, 0, 0);
+          long long emax = 0;
+          int k = 0;
+          if (long_row) {  // gathered by the whole CTA above
+            inf = s_lor[cc];
+            emax = s_lemax;
+            k = n;
           }
+          for (; k + 4 <= n; k += 4) {
+            const int2 q0 = er[k], q1 = er[k + 1], q2 = er[k + 2], q3 = er[k + 3];
+            const uint4 m0 = mask_in[(int64_t)q0.x * L.q4 + col];
+            const uint4 m1 = mask_in[(int64_t)q1.x * L.q4 + col];
+            const uint4 m2 = mask_in[(int64_t)q2.x * L.q4 + col];
+            const uint4 m3 = mask_in[(int64_t)q3.x * L.q4 + col];
+            or4(inf, m0);
+            or4(inf, m1);
+            or4(inf, m2);
+            or4(inf, m3);
+            emax += (long long)q0.y + q1.y + q2.y + q3.y;
+          }
+          for (; k < n; ++k) {
+            const int2 q0 = er[k];
+            or4(inf, mask_in[(int64_t)q0.x * L.q4 + col]);
+            emax += q0.y;
+          }
+#pragma unroll
+          for (int w = 0; w < 4; ++w)
+            X[w] = get4(inf, w) & ~get4(a4, w) & ~get4(b4, w) & word_mask(L, 4 * col + w);
+          efmax = __ll2float_rn(emax);
+          if (scale != 1.0f) efmax = __fmul_rn(efmax, scale);
         }
-        // two pairs of each item per round trip (predicated tails)
-        const int nmax = max(max(nn[0], nn[1]), 0);
-        for (int k = 0; k < nmax; k += 2) {
-          int2 q[2][2];
-          uint4 m[2][2];
+        // ---- queue the exposed words ----
 #pragma unroll
-          for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int j = 0; j < 2; ++j)
-              q[h][j] = k + j < nn[h] ? er[h][k + j] : make_int2(0, 0);
-#pragma unroll
-          for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int j = 0; j < 2; ++j)
-              m[h][j] = k + j < nn[h] ? mask_in[(int64_t)q[h][j].x * L.q4 + cols[h]]
-                                      : make_uint4(0, 0, 0, 0);
-#pragma unroll
-          for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-              or4(inf[h], m[h][j]);
-              emax[h] += q[h][j].y;
-            }
+        for (int w = 0; w < 4; ++w) {
+          const unsigned qm = __ballot_sync(kFull, X[w] != 0u);
+          if (!qm) continue;
+          const int base = Q.n;
+          if (X[w]) {
+            const int pos = base + __popc(qm & ((1u << lane) - 1u));
+            Q.rloc[pos] = rloc;
+            Q.word[pos] = 4 * col + w;
+            Q.X[pos] = X[w];
+            Q.efmax[pos] = efmax;
+          }
+          __syncwarp();
+          if (lane == 0) Q.n = base + __popc(qm);
+          __syncwarp();
         }
-        // the planes only of items with an infectious neighbour
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-          if (nn[h] != 0 && (inf[h].x | inf[h].y | inf[h].z | inf[h].w)) {
-            const int64_t idx = (int64_t)(T.row_begin + rlocs[h]) * L.q4 + cols[h];
-            a4[h] = sa[idx];
-            b4[h] = sb[idx];
+        // ---- decide full rounds (and, past the items, the remainder and
+        // the carried candidates: the staged pairs change with the chunk) ----
+        while (Q.n >= 32 || (flushing && (Q.n > 0 || Q.nk > 0))) {
+          const int take = Q.n < 32 ? Q.n : 32;
+          infect_round(Q, take, flushing && take == Q.n, lane, L, T, cbase, s_rp, s_ent, ent,
+                       staged, e0, s_bw, mask_w, evs_w, flag32, step, scale, c);
+          const int rest = Q.n - take;
+          for (int i = lane; i < rest; i += 32) {
+            Q.rloc[i] = Q.rloc[take + i];
+            Q.word[i] = Q.word[take + i];
+            Q.X[i] = Q.X[take + i];
+            Q.efmax[i] = Q.efmax[take + i];
           }
-        // ---- queue the exposed words of each item, deciding full rounds
-        // after each (and, past the items, the remainder and the carried
-        // candidates: the staged pairs change with the chunk) ----
-#pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-          const uint4 infh = h ? inf[1] : inf[0], ah = h ? a4[1] : a4[0], bh = h ? b4[1] : b4[0];
-          const int colh = h ? cols[1] : cols[0], rloch = h ? rlocs[1] : rlocs[0];
-          const long long emaxh = h ? emax[1] : emax[0];
-          uint32_t X[4] = {0, 0, 0, 0};
-          float efmax = 0.0f;
-          if ((h ? nn[1] : nn[0]) != 0) {
-#pragma unroll
-            for (int w = 0; w < 4; ++w)
-              X[w] = get4(infh, w) & ~get4(ah, w) & ~get4(bh, w) & word_mask(L, 4 * colh + w);
-            efmax = __ll2float_rn(emaxh);
-            if (scale != 1.0f) efmax = __fmul_rn(efmax, scale);
-          }
-#pragma unroll
-          for (int w = 0; w < 4; ++w) {
-            const unsigned qm = __ballot_sync(kFull, X[w] != 0u);
-            if (!qm) continue;
-            const int base = Q.n;
-            if (X[w]) {
-              const int pos = base + __popc(qm & ((1u << lane) - 1u));
-              Q.rloc[pos] = rloch;
-              Q.word[pos] = 4 * colh + w;
-              Q.X[pos] = X[w];
-              Q.efmax[pos] = efmax;
-            }
-            __syncwarp();
-            if (lane == 0) Q.n = base + __popc(qm);
-            __syncwarp();
-          }
-          const bool drain = flushing && h == 1;
-          while (Q.n >= 32 || (drain && (Q.n > 0 || Q.nk > 0))) {
-            const int take = Q.n < 32 ? Q.n : 32;
-            infect_round(Q, take, drain && take == Q.n, lane, L, T, cbase, s_rp, s_ent, ent,
-                         staged, e0, s_beta, s_bw, mask_w, evs_w, flag32, step, scale, c);
-            const int rest = Q.n - take;
-            for (int i = lane; i < rest; i += 32) {
-              Q.rloc[i] = Q.rloc[take + i];
-              Q.word[i] = Q.word[take + i];
-              Q.X[i] = Q.X[take + i];
-              Q.efmax[i] = Q.efmax[take + i];
-            }
-            __syncwarp();
-            if (lane == 0) Q.n = rest;
-            __syncwarp();
-          }
+          __syncwarp();
+          if (lane == 0) Q.n = rest;
+          __syncwarp();
         }
         if (flushing) break;
       }
@@ -761,15 +797,10 @@ __global__ void __launch_bounds__(kThreads, 3)
         rl[h] = in[h] ? (int)dv.div((uint32_t)itv) : 0;
         cl[h] = in[h] ? itv - rl[h] * ncols : 0;
         const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
-        st[h] = in[h] ? flag[idx] : 0;
-      }
-      // the planes of items that may move (an infection event, or replicas
-      // that may be E, I or waning R): the others are skipped unread
-#pragma unroll
-      for (int h = 0; h < kFlowIPL; ++h) {
-        const int64_t idx = (int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h];
         a4[h] = b4[h] = make_uint4(0, 0, 0, 0);
-        if (st[h] & (kFlagEvent | kFlagActive)) {
+        st[h] = 0;
+        if (in[h]) {
+          st[h] = flag[idx];
           a4[h] = sa[idx];
           b4[h] = sb[idx];
         }
@@ -791,9 +822,9 @@ __global__ void __launch_bounds__(kThreads, 3)
         cnt += __popc(cm[h]);
         busy |= (st[h] & kFlagEvent) != 0 || cm[h] != 0;
         // next step's hint byte, from this step's planes and events: a
-        // superset of the items that can move (E, I, waning R, or newly
-        // infected) and of those with susceptible replicas
-        if (st[h] & (kFlagEvent | kFlagActive)) {
+        // superset of the items with susceptible replicas (and of those
+        // that can move: E, I, waning R, or newly infected)
+        if (in[h]) {
           bool act = (st[h] & kFlagEvent) != 0, sus = false;
 #pragma unroll
           for (int w = 0; w < 4; ++w) {
