@@ -614,6 +614,12 @@ rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
     }
     s.step_win[t] = (int32_t)s.wins.size() - 1;
   }
+  // per-item hint bytes pay off on windows with many pairs per row (two per
+  // hit; a window's candidates bound its hits from above): at least 4 N
+  // candidates
+  s.c.hints = 0;
+  for (const WinDesc &d : s.wins)
+    if (d.n_candidates >= 4 * (int64_t)s.N) s.c.hints = 1;
   if (max_cand > (int64_t)INT32_MAX / 2) {
     set_error("a window has %lld candidate contacts; at most 2^30 are supported",
               (long long)max_cand);

@@ -112,7 +112,9 @@ constexpr int kMaxTaskRows = 1024;  // rows of one task (host-side limit)
 // bit 2 replicas that may be susceptible.  k_flow rewrites bits 1-2 of every
 // item from its start-of-step planes and events, as a superset of the next
 // step's state; k_infect skips the neighbours of items without bit 2 where
-// rows are long enough for the extra load to pay.
+// rows are long enough for the extra load to pay.  The hints are kept only
+// for graphs whose windows average at least 8 pairs per row (StepConsts
+// hints); elsewhere the extra work would not pay.
 constexpr uint8_t kFlagEvent = 1, kFlagActive = 2, kFlagSusceptible = 4;
 
 constexpr int kEntCap = 768;        // staged CSR pairs per chunk
@@ -450,11 +452,12 @@ __global__ void __launch_bounds__(kThreads, 3)
       // one row with more pairs than a buffer; streamed only when one of
       // its items may hold susceptible replicas
       const bool long_row =
-          !staged && __syncthreads_or(threadIdx.x < ncols &&
-                                      (flag8[(int64_t)(T.row_begin + r0) * L.q4 + cbase +
-                                             threadIdx.x] & kFlagSusceptible));
+          !staged && (!c.hints ||
+                      __syncthreads_or(threadIdx.x < ncols &&
+                                       (flag8[(int64_t)(T.row_begin + r0) * L.q4 + cbase +
+                                              threadIdx.x] & kFlagSusceptible)));
       const bool skip_row = !staged && !long_row;
-      const bool use_hint = e1 - e0 >= 8 * (r1 - r0);  // at least 8 pairs per row
+      const bool use_hint = c.hints && e1 - e0 >= 8 * (r1 - r0);  // at least 8 pairs per row
       bool dense_done = false;
       if (long_row) {
         // A hub of the window graph.  Its pairs stream through the two halves
@@ -824,7 +827,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         // next step's hint byte, from this step's planes and events: a
         // superset of the items with susceptible replicas (and of those
         // that can move: E, I, waning R, or newly infected)
-        if (in[h]) {
+        if (c.hints && in[h]) {
           bool act = (st[h] & kFlagEvent) != 0, sus = false;
 #pragma unroll
           for (int w = 0; w < 4; ++w) {

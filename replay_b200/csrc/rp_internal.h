@@ -225,6 +225,7 @@ struct StepConsts {
   const float *sus;     // device, may be null
   uint32_t roff;        // replica offset of the stream layout (multiple of 32)
   int32_t *err;         // device flag set by a kernel that gave up a bounded wait
+  int32_t hints;        // batched path: keep and use the per-item hint bytes
 };
 
 // Plain path (column-major N x M state, per-replica SpMV + elementwise).
