@@ -38,10 +38,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sweep", "small", "hot", "quiet"], default="sweep",
+    ap.add_argument("--workload", choices=["sweep", "small", "hot", "quiet", "dense"], default="sweep",
                     help="sweep: the replica-sweep replay (default); small: N=1,000 / 1,000 replicas; "
                          "hot: the sweep network with 5,000 initial infected for 12 steps; quiet: its "
-                         "first 6 steps (profiler cases)")
+                         "first 6 steps; dense: 3 days of the dense stress network (profiler cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain-path / CPU / e2e legs")
     ap.add_argument("--record-traffic", metavar="NCU_CSV",
                     help="store the step kernels' DRAM bytes per step of --workload from an ncu CSV in "
@@ -112,6 +112,15 @@ def workload(name):
     from replay_b200 import synthetic
     if name == "small":
         return synthetic.small_seir()
+    if name == "dense":
+        # the dense stress network's per-window shape (N = 5,000, hub rows of
+        # thousands of pairs, 16,384 replicas) on 3 days of its contacts, with
+        # 5% initially infected so that the hub rows carry infectious replicas
+        net = synthetic.dense_stress(n_contacts=5_000_000, days=3)
+        net["params"] = dict(net["params"], initial_count=250, iterations=48)
+        net["name"] = ("dense stress network, 3 days (5M contacts), N=5000, M=16384, "
+                       "250 initial infected, 48 x 15 min")
+        return net
     net = synthetic.replica_sweep()
     if name == "quiet":
         # the sweep's opening steps, where almost every replica is susceptible
@@ -144,7 +153,7 @@ def profiled_traffic(name):
 def record_traffic(csv_path, workload_name, capture):
     """Reads an ncu CSV (`ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
     ... --csv`) and stores the DRAM bytes per step (k_infect + k_flow, one
-    launch each, averaged over the captured steps) of the workload in
+    launch each, averaged over the first replay's steps) of the workload in
     profiles/traffic.json."""
     import csv
     with open(csv_path) as f:
@@ -162,7 +171,11 @@ def record_traffic(csv_path, workload_name, capture):
             per_launch.setdefault(k, {})[r["ID"]] = per_launch.get(k, {}).get(r["ID"], 0.0) + val * scale
     if not per_launch.get("k_infect") or not per_launch.get("k_flow"):
         raise SystemExit(f"no k_infect / k_flow DRAM metrics in {csv_path}")
-    inf, flo = list(per_launch["k_infect"].values()), list(per_launch["k_flow"].values())
+    steps = int(workload(workload_name)["params"]["iterations"])
+    order = lambda d: [d[k] for k in sorted(d, key=int)][:steps]  # launch order, one replay
+    inf, flo = order(per_launch["k_infect"]), order(per_launch["k_flow"])
+    if len(inf) < steps or len(flo) < steps:
+        raise SystemExit(f"{csv_path} holds {len(inf)} / {len(flo)} step launches, not {steps}")
     rows = [a + b for a, b in zip(inf, flo)]
     try:
         with open(TRAFFIC_JSON) as f:
@@ -408,13 +421,18 @@ def dense_stress_leg(replay_b200, dev, timed, hbm):
     bytes_replay = algorithmic_bytes(n, M, T, nnz_total)
     launch_ms = prof["spmv_ms"] / max(1, prof["spmv_launches"]) + prof["step_ms"] / max(1, prof["step_launches"])
     achieved = (bytes_replay / T) / (launch_ms / 1e3) / 1e9
+    # DRAM bytes per step of the same kernels on 3 days of this network (the
+    # `dense` workload: same N, M and window shape, hence the same per-step
+    # state and CSR sizes)
+    traffic, capture = profiled_traffic("dense")
     g.close()
     return {"workload": net["name"], "contacts": int(len(net["start"])), "ingest_s": ingest,
             "ms_per_replay": ms, "value": n * M * T / (ms / 1e3), "unit": UNIT,
             "nnz_per_step": nnz_total / T,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "kernel": "k_infect + k_flow", "algorithmic_bytes_per_launch": bytes_replay / T,
-                         "avg_launch_us": launch_ms * 1e3,
+                         "avg_launch_us": launch_ms * 1e3, "traffic": traffic,
+                         "traffic_source": f"profiles/traffic.json: {capture}" if capture else None,
                          "note": "the 10 MB infectious mask stays in L2: algorithmic gather bytes exceed DRAM traffic"}}
 
 

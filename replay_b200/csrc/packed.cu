@@ -174,6 +174,7 @@ __device__ __forceinline__ int pair_shift(const int2 *ent, int32_t k0) {
 // Per-warp queue of exposed words of k_infect (dynamic shared memory):
 // entries accumulate over rows and are decided 32 at a time.
 constexpr int kInfectQueue = 160;  // 31 left over + 4 words x 32 lanes of one pass
+constexpr int kWordExact = 4;      // candidates of a word (long row) for the one-pass exact test
 struct InfectQueue {
   uint4 pl[32][2];               // the 8 random planes of each word (round scratch)
   int32_t rloc[kInfectQueue];    // task-relative row
@@ -206,12 +207,86 @@ __device__ __forceinline__ uint32_t queued_top8(const uint4 (&q)[2], uint32_t b)
   return top8_of(pl, b);
 }
 
+// What an infection decision reads besides the candidate (values, so that
+// the out-of-line word_exact_pass takes them in registers).
+struct DecideArgs {
+  const uint32_t *rk;     // Philox round keys
+  const float *beta_r;    // per-replica beta, or null
+  const float *sus;       // per-node susceptibility, or null
+  float beta, scale;
+  uint32_t roff, step;
+  int32_t words, q4, row_begin;
+};
+
+// Decides candidate replica b of task-relative row orl, word `word`, from
+// its exact exposure e (contact-seconds) and its uniform's top byte u8.
+__device__ __forceinline__ void decide(const DecideArgs &d, int orl, int word, int b,
+                                       long long e, uint32_t u8, uint32_t *evs_w,
+                                       uint32_t *flag32) {
+  const int orow = d.row_begin + orl;
+  const float br = d.beta_r ? __ldg(d.beta_r + word * 32 + b) : d.beta;
+  const float bs = d.sus ? __fmul_rn(br, d.sus[orow]) : br;
+  float ef = __ll2float_rn(e);
+  if (d.scale != 1.0f) ef = __fmul_rn(ef, d.scale);
+  const float xx = __fmul_rn(bs, ef);
+  if (!(xx > 0.0f)) return;
+  // P <= x: a uniform whose top byte is above x's cannot infect (no
+  // exponential)
+  if (xx < 1.0f && u8 > (uint32_t)(fixed64(xx) >> 56)) return;
+  const uint32_t gword = (uint32_t)word + (d.roff >> 5);
+  if (infect_event(one_minus_exp_neg(xx), u8, d.rk, (uint32_t)orow, d.step,
+                   gword * 32u + (uint32_t)b)) {
+    atomicOr(&evs_w[(int64_t)orow * d.words + word], 1u << b);
+    const int64_t idx = (int64_t)orow * d.q4 + (word >> 2);
+    atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
+  }
+}
+
+// The exact test of the queued words in `wlist` (lane o's word holds
+// candidates Cw of lane o): one pass over each word's row with lane =
+// replica, so that each pair's mask word is one broadcast load shared by all
+// the word's candidates.  For words with many candidates on rows of more
+// than 32 pairs (a dense neighbourhood, whose bound test lets most exposed
+// replicas through); on other words the per-replica test costs less.  Kept
+// out of line: the busy steps of sparse graphs rarely take it.
+__device__ __noinline__ void word_exact_pass(const InfectQueue &Q, unsigned wlist, uint32_t Cw,
+                                             int lane, const int32_t *s_rp, const int2 *s_ent,
+                                             const int2 *__restrict__ ent, bool staged, int32_t e0,
+                                             const uint32_t *mask_w, uint32_t *evs_w,
+                                             uint32_t *flag32, DecideArgs d) {
+  for (unsigned t = wlist; t; t &= t - 1) {
+    const int o = __ffs(t) - 1;
+    const uint32_t Co = __shfl_sync(kFull, Cw, o);
+    const int orl = Q.rloc[o], word = Q.word[o];
+    const int32_t kend = s_rp[orl + 1];
+    int32_t k = s_rp[orl];
+    long long e = 0;
+    for (; k + 4 <= kend; k += 4) {
+      int2 q[4];
+      uint32_t m[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) q[j] = staged ? s_ent[k + j - e0] : __ldg(ent + k + j);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) m[j] = mask_w[(int64_t)q[j].x * d.words + word];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) e += ((m[j] >> lane) & 1u) ? q[j].y : 0;
+    }
+    for (; k < kend; ++k) {
+      const int2 q0 = staged ? s_ent[k - e0] : __ldg(ent + k);
+      e += ((mask_w[(int64_t)q0.x * d.words + word] >> lane) & 1u) ? q0.y : 0;
+    }
+    if ((Co >> lane) & 1u)
+      decide(d, orl, word, lane, e, queued_top8(Q.pl[o], (uint32_t)lane), evs_w, flag32);
+  }
+}
+
 // Decides up to 32 queued exposed words: the bound test one word per lane
-// (phase 2), then the exact test of the surviving candidates one replica
-// per lane (phase 3), in full batches of 32 together with the candidates
-// carried from earlier rounds; fewer than 32 left over are carried to the
-// next round unless `drain` is set.  Events are OR-ed into their words and
-// flag their items.
+// (phase 2), then the exact test of the surviving candidates: a word with
+// at least kWordExact of them in one pass over its row (phase 3a), the
+// others one replica per lane (phase 3), in full batches of 32 together with
+// the candidates carried from earlier rounds; fewer than 32 left over are
+// carried to the next round unless `drain` is set.  Events are OR-ed into
+// their words and flag their items.
 __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, int lane,
                                              const PackedLayout &L, const PackedTask &T,
                                              int cbase, const int32_t *s_rp, const int2 *s_ent,
@@ -238,6 +313,14 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
       Q.pl[lane][1] = make_uint4(pl[4], pl[5], pl[6], pl[7]);
     }
   }
+  // ---- phase 3a: a word with many candidates on a row of more than 32
+  // pairs takes one pass over its row (word_exact_pass) ----
+  const unsigned wlist = __ballot_sync(
+      kFull, __popc(Cw) >= kWordExact && s_rp[Q.rloc[lane] + 1] - s_rp[Q.rloc[lane]] > 32);
+  const DecideArgs d{c.rk, c.beta_r, c.sus, c.beta, scale, c.roff, step, L.words, L.q4,
+                     T.row_begin};
+  if (wlist) word_exact_pass(Q, wlist, Cw, lane, s_rp, s_ent, ent, staged, e0, mask_w, evs_w, flag32, d);
+  if ((wlist >> lane) & 1u) Cw = 0;
   Q.C[lane] = Cw;
   int ctotal;
   Q.off[lane] = warp_excl_scan(__popc(Cw), lane, ctotal);
@@ -329,24 +412,7 @@ __device__ __forceinline__ void infect_round(InfectQueue &Q, int n, bool drain, 
     __syncwarp();
     e = Q.esum[lane];
     }
-    if (p >= total) continue;
-    const int orow = T.row_begin + orl;
-    const float br = c.beta_r ? __ldg(c.beta_r + word * 32 + b) : c.beta;
-    const float bs = c.sus ? __fmul_rn(br, c.sus[orow]) : br;
-    float ef = __ll2float_rn(e);
-    if (scale != 1.0f) ef = __fmul_rn(ef, scale);
-    const float xx = __fmul_rn(bs, ef);
-    if (!(xx > 0.0f)) continue;
-    // P <= x: a uniform whose top byte is above x's cannot infect (no
-    // exponential)
-    if (xx < 1.0f && u8 > (uint32_t)(fixed64(xx) >> 56)) continue;
-    const uint32_t gword = (uint32_t)word + (c.roff >> 5);
-    if (infect_event(one_minus_exp_neg(xx), u8, c.rk, (uint32_t)orow, step,
-                     gword * 32u + (uint32_t)b)) {
-      atomicOr(&evs_w[(int64_t)orow * L.words + word], 1u << b);
-      const int64_t idx = (int64_t)orow * L.q4 + (word >> 2);
-      atomicOr(&flag32[idx >> 2], 1u << (8 * (idx & 3)));
-    }
+    if (p < total) decide(d, orl, word, b, e, u8, evs_w, flag32);
   }
   __syncwarp();
   // carry the rest: slots below nk keep their entries when no batch ran
@@ -375,7 +441,8 @@ __global__ void __launch_bounds__(kThreads, 3)
              const int32_t *__restrict__ row_ptr, const int2 *__restrict__ ent,
              const uint4 *__restrict__ mask_in, const uint4 *__restrict__ sa,
              const uint4 *__restrict__ sb, uint4 *__restrict__ evs,
-             uint32_t *__restrict__ flag32, uint32_t step, float scale, StepConsts c) {
+             uint32_t *__restrict__ flag32, uint32_t step, float scale,
+             const __grid_constant__ StepConsts c) {
   __shared__ int32_t s_rp[kMaxTaskRows + 1];
   __shared__ float s_bw[128];  // max |beta_r| of each word of the slice
   __shared__ uint4 s_lor[32];  // long row: OR of the neighbours' masks per column

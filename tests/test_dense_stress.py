@@ -52,6 +52,26 @@ def test_reduced_dense_stress_matches_oracle(rb, oracle, csr):
     assert got[-1, :, 2].sum() > 0  # recoveries happened
 
 
+@pytest.mark.parametrize("csr", ["per-step", "prebuilt"])
+def test_dense_neighbourhoods_match_oracle(rb, oracle, csr):
+    """Five percent initially infected on the dense network: in the first
+    steps most susceptible replicas of a row are exposed with an infection
+    bound near 1, so whole words reach the exact test (the one-pass word
+    test as well as the per-replica one)."""
+    net = synthetic.dense_stress(seed=6, n_contacts=1_666_667, days=1, steps=96, replicas=64)
+    kw = dict(net["params"], M=64, iterations=24, initial_count=250, seed=13)
+    g = _graph(rb, net)
+    got = rb.Simulation(g, path="batched", csr=csr, **kw).run()
+    want = oracle.run(net["start"], net["end"], net["u"], net["v"], net["n_nodes"], n_replicas=64,
+                      n_steps=24, step_size=kw["step_size"], window=kw["window"],
+                      start_time=kw["start_time"], transition=1, beta=kw["beta"], p_ir=kw["p_ir"],
+                      has_exposed=0, initial_count=250, seed=13)
+    np.testing.assert_array_equal(got, want)
+    # the epidemic takes off in every replica from the first steps
+    assert (got[0, :, 3] - got[2, :, 3]).min() > 0
+    assert (got[0, :, 3] - got[2, :, 3]).mean() > 20
+
+
 def test_full_dense_stress_properties_and_shard(rb):
     net = synthetic.dense_stress()
     p = dict(net["params"])
