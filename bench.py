@@ -38,10 +38,12 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sweep", "small", "hot", "quiet", "dense"], default="sweep",
+    ap.add_argument("--workload", choices=["sweep", "small", "hot", "quiet", "dense", "uneven"],
+                    default="sweep",
                     help="sweep: the replica-sweep replay (default); small: N=1,000 / 1,000 replicas; "
                          "hot: the sweep network with 5,000 initial infected for 12 steps; quiet: its "
-                         "first 6 steps; dense: 3 days of the dense stress network (profiler cases)")
+                         "first 6 steps; dense: 3 days of the dense stress network; uneven: 32 "
+                         "networks of the uneven batch for 96 steps (profiler cases)")
     ap.add_argument("--no-extras", action="store_true", help="skip plain-path / CPU / e2e legs")
     ap.add_argument("--record-traffic", metavar="NCU_CSV",
                     help="store the step kernels' DRAM bytes per step of --workload from an ncu CSV in "
@@ -112,6 +114,15 @@ def workload(name):
     from replay_b200 import synthetic
     if name == "small":
         return synthetic.small_seir()
+    if name == "uneven":
+        # the uneven batch's network mix (N log-uniform in 500..50,000, 128
+        # replicas each) on 32 networks for 96 steps, batched into one replay
+        from replay_b200 import batch_networks
+        b = synthetic.uneven_batch(n_networks=32)
+        s, e, u, v, n, off = batch_networks(b["networks"])
+        return dict(start=s, end=e, u=u, v=v, n_nodes=n, net_first=off,
+                    params=dict(b["params"], iterations=96),
+                    name="uneven batch sample: 32 networks, N log-uniform 500..50k, 96 x 30 min, M=128 each")
     if name == "dense":
         # the dense stress network's per-window shape (N = 5,000, hub rows of
         # thousands of pairs, 16,384 replicas) on 3 days of its contacts, with
@@ -226,7 +237,8 @@ def run_ours(args, rank, world, local_rank):
     t0 = time.perf_counter()
     g = replay_b200.Graph.from_arrays(net["start"], net["end"], net["u"], net["v"], n_nodes, device=dev)
     ingest_s = time.perf_counter() - t0
-    sim = replay_b200.Simulation(g, path="batched", csr="per-step", **p)
+    nets = {"networks": net["net_first"]} if "net_first" in net else {}
+    sim = replay_b200.Simulation(g, path="batched", csr="per-step", **nets, **p)
     info = sim.info
 
     stream = torch.cuda.Stream(device=dev)
@@ -270,7 +282,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- prebuilt-CSR variant (with --no-extras only built, for its nnz count,
     # after the per-step replays, so that those are the process's first launches) ----
     prof_ps = sim.profile() if args.no_extras else None
-    sim_pre = replay_b200.Simulation(g, path="batched", csr="prebuilt", **p)
+    sim_pre = replay_b200.Simulation(g, path="batched", csr="prebuilt", **nets, **p)
     nnz_total = sim_pre.info["nnz_total"]
     if not args.no_extras:
         ms_pre = timed(sim_pre, args.steps, 1) / args.steps

@@ -845,7 +845,13 @@ __global__ void __launch_bounds__(kThreads, 3)
     const int ncols = min(32, L.q4 - cbase);
     const Div dv((uint32_t)ncols);
     const int nrows = T.row_end - T.row_begin;
-    for (int j = threadIdx.x; j < 128 * 32; j += blockDim.x) s_ev[j] = 0;
+    {  // the task's counters: two 32-bit words for each of its ncols x 128 replicas
+      uint32_t *c0 = reinterpret_cast<uint32_t *>(s_ev);
+      for (int j = threadIdx.x; j < ncols * 128; j += blockDim.x) {
+        c0[j] = 0;
+        c0[128 * 32 + j] = 0;
+      }
+    }
     if (lane == 0) Q.n = 0;
     __syncthreads();
     const int nitems = nrows * ncols;
@@ -884,10 +890,9 @@ __global__ void __launch_bounds__(kThreads, 3)
       for (int h = 0; h < kFlowIPL; ++h) {
         cm[h] = 0;
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
+        for (int w = 0; w < 4; ++w) {  // padding replicas are S: no replica mask needed
           const uint32_t A = get4(a4[h], w), B = get4(b4[h], w);
-          const bool valid = in[h] && word_mask(L, 4 * (cbase + cl[h]) + w) != 0u;
-          if (valid && (waning ? (A | B) : (A ^ B)) != 0u) cm[h] |= 1u << w;
+          if ((waning ? (A | B) : (A ^ B)) != 0u) cm[h] |= 1u << w;
         }
         cnt += __popc(cm[h]);
         busy |= (st[h] & kFlagEvent) != 0 || cm[h] != 0;
@@ -895,16 +900,19 @@ __global__ void __launch_bounds__(kThreads, 3)
         // superset of the items with susceptible replicas (and of those
         // that can move: E, I, waning R, or newly infected)
         if (c.hints && in[h]) {
-          bool act = (st[h] & kFlagEvent) != 0, sus = false;
+          // E, I or waning R (the words of cm), or an infection event
+          const bool act = (st[h] & kFlagEvent) != 0 || cm[h] != 0u;
+          uint32_t s4 = 0;
 #pragma unroll
           for (int w = 0; w < 4; ++w) {
             const uint32_t A = get4(a4[h], w), B = get4(b4[h], w);
-            const uint32_t vm = word_mask(L, 4 * (cbase + cl[h]) + w);
-            act |= (((A ^ B) | (waning ? (A & B) : 0u)) & vm) != 0u;
-            // S now, or back to S this step (waning R, or I -> S)
-            sus |= ((~A & ~B) | (waning ? (A & B) : 0u) | (c.ir_to_s ? (A & ~B) : 0u)) & vm;
+            // S now, or back to S this step (waning R, or I -> S); padding
+            // replicas are S, so only a row's last item needs the mask
+            uint32_t sw = (~A & ~B) | (waning ? (A & B) : 0u) | (c.ir_to_s ? (A & ~B) : 0u);
+            if (4 * (cbase + cl[h]) + 4 > L.vwords) sw &= word_mask(L, 4 * (cbase + cl[h]) + w);
+            s4 |= sw;
           }
-          const uint8_t nb = (uint8_t)((act ? kFlagActive : 0) | (sus ? kFlagSusceptible : 0));
+          const uint8_t nb = (uint8_t)((act ? kFlagActive : 0) | (s4 ? kFlagSusceptible : 0));
           if (nb != st[h]) flag[(int64_t)(T.row_begin + rl[h]) * L.q4 + cbase + cl[h]] = nb;
         }
       }
@@ -936,15 +944,25 @@ __global__ void __launch_bounds__(kThreads, 3)
       int pos = warp_excl_scan(cnt, lane, total);
       if (total > 0) {  // warp-uniform
         pos += Q.n;
+        // one iteration per candidate word of the lane (most lanes have none)
+        uint32_t all = 0;
 #pragma unroll
-        for (int h = 0; h < kFlowIPL; ++h)
+        for (int h = 0; h < kFlowIPL; ++h) all |= cm[h] << (4 * h);
+        while (all) {
+          const int bit = __ffs(all) - 1;
+          all &= all - 1;
+          const int h = bit >> 2;
+          int r = rl[0], cc = cl[0];
 #pragma unroll
-          for (int w = 0; w < 4; ++w)
-            if ((cm[h] >> w) & 1u) {
-              Q.row[pos] = T.row_begin + rl[h];
-              Q.word[pos] = (uint16_t)(4 * (cbase + cl[h]) + w);
-              ++pos;
+          for (int hh = 1; hh < kFlowIPL; ++hh)
+            if (h == hh) {
+              r = rl[hh];
+              cc = cl[hh];
             }
+          Q.row[pos] = T.row_begin + r;
+          Q.word[pos] = (uint16_t)(4 * (cbase + cc) + (bit & 3));
+          ++pos;
+        }
         __syncwarp();
       }
       const int n = Q.n + total;
@@ -1000,7 +1018,7 @@ __global__ void __launch_bounds__(kThreads)
     const PackedTask T = tasks[ti];
     const int wbase = T.slice * 128;
     const int nw = min(128, L.words - wbase);
-    for (int j = threadIdx.x; j < 128 * 32; j += blockDim.x) s_ev[j] = 0;
+    for (int j = threadIdx.x; j < nw * 32; j += blockDim.x) s_ev[j] = 0;
     __syncthreads();
     const int64_t items = (int64_t)(T.row_end - T.row_begin) * nw;
     for (int64_t it = threadIdx.x; it < items; it += blockDim.x) {
