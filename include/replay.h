@@ -9,10 +9,14 @@
  * defaults and CSV outputs and is implemented on top of these calls.
  *
  * Conventions: plain pointers and sizes, no C++ or torch types; every call
- * returns an rp_status (no exit(), no process-wide state); rp_last_error()
- * describes the last failure on the calling thread.  Handles are not
- * thread-safe; distinct handles may be used from distinct threads.  Device
- * memory is owned by the handle; host arrays are owned by the caller.
+ * returns an rp_status (no exit()); rp_last_error() describes the last
+ * failure on the calling thread.  Handles are not thread-safe; distinct
+ * handles may be used from distinct threads.  Device memory is owned by the
+ * handle; host arrays are owned by the caller.  The one process-wide state
+ * is a thread-safe cache of device blocks: freeing a graph, simulation or
+ * mean-field handle synchronizes the device and keeps its blocks (up to
+ * 8 GiB per device) for the next handle instead of returning them with
+ * cudaFree; rp_release_cached_memory() returns them.
  */
 #ifndef REPLAY_H
 #define REPLAY_H
@@ -45,6 +49,9 @@ typedef enum {
 RP_API const char *rp_last_error(void);
 /* Library version string. */
 RP_API const char *rp_version(void);
+/* Returns every device block kept from freed handles to the driver
+ * (cudaFree), on every device.  No reference counterpart. */
+RP_API void rp_release_cached_memory(void);
 
 /* ------------------------------------------------------------------------ */
 /* Contact graphs.                                                           */

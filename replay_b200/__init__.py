@@ -24,11 +24,18 @@ from . import _lib
 from ._lib import CLI_PATH, ReplayError, check, lib
 
 __all__ = ["Graph", "Simulation", "ReplayError", "window_csr", "parse_contacts", "batch_networks", "CLI_PATH",
-           "version"]
+           "version", "release_cached_memory"]
 
 
 def version():
     return lib().rp_version().decode()
+
+
+def release_cached_memory():
+    """Returns the device blocks kept from closed graphs and simulations
+    (closing a handle keeps its blocks, up to 8 GiB per device, for the
+    next one) to the driver."""
+    lib().rp_release_cached_memory()
 
 
 def _ptr(a):

@@ -88,6 +88,7 @@ TEXT_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_c
 SIGNATURES = {
     "rp_last_error": ([], C.c_char_p),
     "rp_version": ([], C.c_char_p),
+    "rp_release_cached_memory": ([], None),
     "rp_graph_load_text": ([C.c_char_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "rp_graph_from_arrays": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int,
                               C.POINTER(C.c_void_p)], C.c_int),

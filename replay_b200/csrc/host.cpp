@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -34,6 +35,80 @@ rp_status cuda_fail(cudaError_t e, const char *what) {
   set_error("%s: %s", what, cudaGetErrorString(e));
   (void)cudaGetLastError();
   return RP_ERR_CUDA;
+}
+
+// ---- kept device blocks ------------------------------------------------------
+thread_local int g_park = 0;
+
+namespace {
+struct KeptBlock {
+  int device;
+  size_t cap;
+  void *ptr;
+};
+std::mutex g_cache_mu;
+std::vector<KeptBlock> g_cache;  // oldest first
+
+// cudaFree on the block's own device, restoring the caller's device
+void free_on(int device, void *p) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != device) cudaSetDevice(device);
+  cudaFree(p);
+  if (cur != device) cudaSetDevice(cur);
+}
+}  // namespace
+
+void *cache_take(int device, size_t n, size_t *cap) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  size_t best = g_cache.size();
+  for (size_t i = 0; i < g_cache.size(); ++i) {
+    const KeptBlock &b = g_cache[i];
+    if (b.device != device || b.cap < n || b.cap / 2 > n) continue;
+    if (best == g_cache.size() || b.cap < g_cache[best].cap) best = i;
+  }
+  if (best == g_cache.size()) return nullptr;
+  void *p = g_cache[best].ptr;
+  *cap = g_cache[best].cap;
+  g_cache.erase(g_cache.begin() + (std::ptrdiff_t)best);
+  return p;
+}
+
+void cache_put(int device, void *p, size_t cap) {
+  std::vector<KeptBlock> evict;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    g_cache.push_back(KeptBlock{device, cap, p});
+    size_t kept = 0;
+    for (const KeptBlock &b : g_cache)
+      if (b.device == device) kept += b.cap;
+    for (size_t i = 0; i < g_cache.size() && kept > kCacheBytes;) {
+      if (g_cache[i].device == device) {
+        kept -= g_cache[i].cap;
+        evict.push_back(g_cache[i]);
+        g_cache.erase(g_cache.begin() + (std::ptrdiff_t)i);
+      } else {
+        ++i;
+      }
+    }
+  }
+  for (const KeptBlock &b : evict) free_on(b.device, b.ptr);
+}
+
+void cache_trim(int device) {
+  std::vector<KeptBlock> out;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (size_t i = 0; i < g_cache.size();) {
+      if (device < 0 || g_cache[i].device == device) {
+        out.push_back(g_cache[i]);
+        g_cache.erase(g_cache.begin() + (std::ptrdiff_t)i);
+      } else {
+        ++i;
+      }
+    }
+  }
+  for (const KeptBlock &b : out) free_on(b.device, b.ptr);
 }
 
 namespace {
@@ -184,6 +259,9 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 }  // namespace
 
 struct rp_sim {
+  // destroyed after every buffer below: armed by the destructor once the
+  // device is idle, so that the buffers are kept for reuse
+  ParkGuard park;
   const Graph *g = nullptr;
   rp_params p{};
   int path = RP_PATH_PLAIN;
@@ -255,6 +333,11 @@ struct rp_sim {
     }
     if (text_len_host) cudaFreeHost(text_len_host);
     if (stream) cudaStreamDestroy(stream);
+    // work enqueued on a caller's stream may still read the buffers: the
+    // wait cudaFree would have made
+    if (g && cudaSetDevice(g->device) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess)
+      park.arm();
+    (void)cudaGetLastError();
   }
 
   // Node-state CSV lines of one recorded step, formatted on the device in
@@ -477,6 +560,7 @@ struct rp_sim {
 // Mean-field replay: the schedule and prebuilt window CSRs of a geometric
 // simulation, FP32 probability planes, checkpoints every K steps.
 struct rp_meanfield {
+  ParkGuard park;  // destroyed last (see rp_sim)
   rp_sim base;
   int32_t N = 0, T = 0, K = 24, nblk = 0, n_ckpt = 0;
   MfRates rates{};
@@ -501,6 +585,8 @@ struct rp_meanfield {
     if (fwd) cudaGraphExecDestroy(fwd);
     if (bwd) cudaGraphExecDestroy(bwd);
     if (cap) cudaStreamDestroy(cap);
+    if (cudaDeviceSynchronize() == cudaSuccess) park.arm();
+    (void)cudaGetLastError();
   }
 };
 
@@ -917,6 +1003,7 @@ extern "C" {
 
 RP_API const char *rp_last_error(void) { return g_err; }
 RP_API const char *rp_version(void) { return "replay-b200 0.1 (sm_100a)"; }
+RP_API void rp_release_cached_memory(void) { cache_trim(-1); }
 
 RP_API rp_status rp_graph_load_text(const char *path, int device, rp_graph **out) {
   if (!path || !out) {

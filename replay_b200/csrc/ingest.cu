@@ -316,8 +316,8 @@ rp_status radix_sort(DevBuf &key, DevBuf &val, DevBuf &k2, DevBuf &v2, int64_t n
     k_digit_scatter<<<n_tiles, kSortThreads, 0, st>>>(
         key.as<unsigned long long>(), val.as<uint32_t>(), n, shift, n_tiles, offs.as<int32_t>(),
         k2.as<unsigned long long>(), v2.as<uint32_t>());
-    std::swap(key.ptr, k2.ptr);
-    std::swap(val.ptr, v2.ptr);
+    key.swap(k2);
+    val.swap(v2);
   }
   RP_TRY_CUDA(cudaGetLastError());
   return RP_OK;
@@ -345,6 +345,8 @@ rp_status graph_build_device(Graph &g, const int64_t *start, const int64_t *end,
   g.h_cs.clear();
   if (n == 0) return RP_OK;
   cudaStream_t st = nullptr;
+  // the scratch below is kept for the next build once the stream is idle
+  ParkGuard park;
   DevBuf s, e, uu, vv, key, val, k2, v2, counts, offs, sums, mm, ctr, agg, ss, se, su, sv;
   RP_TRY(s.alloc(sizeof(int64_t) * n));
   RP_TRY(e.alloc(sizeof(int64_t) * n));
@@ -441,6 +443,7 @@ rp_status graph_build_device(Graph &g, const int64_t *start, const int64_t *end,
   RP_TRY_CUDA(cudaMemcpyAsync(g.h_cs.data(), g.cs.ptr, sizeof(int64_t) * n, cudaMemcpyDeviceToHost,
                               st));
   RP_TRY_CUDA(cudaStreamSynchronize(st));
+  park.arm();
   g.nlists = ((int64_t)hc[0] - 1) + (int64_t)hc[1];
   for (int c = 0; c < kClasses; ++c) {
     g.class_off[c + 1] = g.class_off[c] + (int64_t)hc[2 + c];

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <cstdlib>
 #include <vector>
 
@@ -31,9 +32,45 @@ rp_status cuda_fail(cudaError_t e, const char *what);
   } while (0)
 
 // ---- device buffer ----------------------------------------------------------
+// Device blocks released while no device work can touch them are kept for
+// reuse instead of going back through cudaFree, whose device-wide wait and
+// unmapping dominate closing a simulation or a graph and whose matching
+// cudaMalloc calls dominate creating the next one.  An owner parks its
+// buffers (ParkGuard) after synchronizing the device; DevBuf::alloc takes
+// the smallest kept block of the current device that fits (at most twice
+// the request); a failing cudaMalloc returns that device's kept blocks and
+// retries.  At most kCacheBytes stay kept per device (the oldest go first);
+// rp_release_cached_memory returns them all.
+constexpr size_t kCacheBytes = size_t(8) << 30;
+void *cache_take(int device, size_t n, size_t *cap);
+void cache_put(int device, void *p, size_t cap);
+void cache_trim(int device);  // -1: every device
+extern thread_local int g_park;  // > 0: releases on this thread keep their blocks
+
+// Declared before the buffers it covers (so it is destroyed after them) and
+// armed once the device work that used them has completed: from then on the
+// buffers released on this thread are kept instead of freed.
+struct ParkGuard {
+  bool armed = false;
+  ParkGuard() = default;
+  ParkGuard(const ParkGuard &) = delete;
+  ParkGuard &operator=(const ParkGuard &) = delete;
+  void arm() {
+    if (!armed) {
+      armed = true;
+      ++g_park;
+    }
+  }
+  ~ParkGuard() {
+    if (armed) --g_park;
+  }
+};
+
 struct DevBuf {
   void *ptr = nullptr;
   size_t bytes = 0;
+  size_t cap = 0;     // bytes of the block behind ptr (>= bytes)
+  int dev = 0;        // device of the block
   bool owned = true;  // false: a view of memory this buffer must not free
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
@@ -42,7 +79,22 @@ struct DevBuf {
   rp_status alloc(size_t n) {
     release();
     if (n == 0) n = 16;
+    int d = 0;
+    cudaGetDevice(&d);
+    size_t c = 0;
+    if (void *p = cache_take(d, n, &c)) {
+      ptr = p;
+      bytes = n;
+      cap = c;
+      dev = d;
+      return RP_OK;
+    }
     cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      cache_trim(d);
+      e = cudaMalloc(&ptr, n);
+    }
     if (e != cudaSuccess) {
       ptr = nullptr;
       (void)cudaGetLastError();
@@ -50,13 +102,31 @@ struct DevBuf {
       return RP_ERR_NOMEM;
     }
     bytes = n;
+    cap = n;
+    dev = d;
     return RP_OK;
   }
   void release() {
-    if (ptr && owned) cudaFree(ptr);
+    if (ptr && owned) {
+      if (g_park > 0)
+        cache_put(dev, ptr, cap);
+      else
+        cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
+    cap = 0;
     owned = true;
+  }
+  // Exchanges the blocks of two buffers (pointer, sizes, device, ownership:
+  // a block's size must travel with it, or it would be kept under the wrong
+  // size).
+  void swap(DevBuf &o) {
+    std::swap(ptr, o.ptr);
+    std::swap(bytes, o.bytes);
+    std::swap(cap, o.cap);
+    std::swap(dev, o.dev);
+    std::swap(owned, o.owned);
   }
   // Points at memory owned elsewhere (no allocation; release() won't free it).
   void borrow(void *p, size_t n) {
@@ -313,6 +383,12 @@ void plain_spmv_f32_raw(const int32_t *row_ptr, const int32_t *col,
 }  // namespace rp
 
 struct rp_graph {
+  rp::ParkGuard park;  // destroyed after g: its blocks are kept for reuse
   rp::Graph g;
   double prep_ms = 0.0, build_ms = 0.0;  // creation phases (rp_graph_info)
+  ~rp_graph() {
+    if (cudaSetDevice(g.device) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess)
+      park.arm();
+    (void)cudaGetLastError();
+  }
 };
