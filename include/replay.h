@@ -301,7 +301,7 @@ RP_API rp_status rp_sim_profile_steps(rp_sim *s, float *step_ms);
 
 /* Tile autotuner of the batched path (no reference counterpart).  Networks
  * are bucketed by size (floor(log2 nodes)); for each bucket, largest first,
- * the task height (rows of one task: 32..1024) is chosen by timing the
+ * the task height (rows of one task: 32..4096) is chosen by timing the
  * replay's first `probe_steps` steps with CUDA events, keeping a candidate
  * only when it is 2% faster.  The simulation keeps the tuned tiles (and
  * re-captures its CUDA graph); results are unchanged by tiling.  Not for

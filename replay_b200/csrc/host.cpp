@@ -763,13 +763,16 @@ rp_status sim_setup(rp_sim &s, const Graph &g, const rp_params &p) {
   return RP_OK;
 }
 
-// Rows per batched task: about one wave of CTAs (148 SMs x 3), at most 1024
-// rows (the kernels stage a task's row pointers in shared memory).
+// Rows per batched task: about one wave of CTAs (148 SMs x 3), between 32
+// and 4,096 rows (a task stages its row pointers in shared memory).  Sparse
+// batches of many networks reach the cap: there a task is a short chain of
+// global round trips, and fewer, taller tasks shorten the step.
+constexpr int64_t kTaskRowsDefaultMax = 4096;
 int32_t rows_per_task(int32_t n_rows, int32_t n_slices) {
   const int64_t target_tasks = 148 * 3;
   int64_t rows = ((int64_t)n_rows * n_slices + target_tasks - 1) / target_tasks;
   if (rows < 32) rows = 32;
-  if (rows > 1024) rows = 1024;
+  if (rows > kTaskRowsDefaultMax) rows = kTaskRowsDefaultMax;
   return (int32_t)rows;
 }
 
@@ -791,6 +794,9 @@ rp_status upload_tasks(rp_sim &s) {
   RP_TRY_CUDA(cudaMemcpy(s.tasks.ptr, tasks.data(), sizeof(PackedTask) * tasks.size(),
                          cudaMemcpyHostToDevice));
   s.L.n_tasks = (int32_t)tasks.size();
+  s.L.max_task_rows = 0;
+  for (const PackedTask &t : tasks)
+    s.L.max_task_rows = std::max(s.L.max_task_rows, t.row_end - t.row_begin);
   return RP_OK;
 }
 
@@ -1557,7 +1563,7 @@ RP_API rp_status rp_sim_autotune(rp_sim *s, int32_t probe_steps, rp_tune_result 
   double best = 0.0;
   rp_status st = time_probe(best);
   const double ms_default = best;
-  static const int32_t kCand[] = {32, 64, 128, 256, 512, 1024};
+  static const int32_t kCand[] = {32, 64, 128, 256, 512, 1024, 2048, 4096};
   std::vector<int32_t> chosen(blist.size(), 0);
   for (size_t bi = 0; bi < blist.size() && st == RP_OK; ++bi) {
     std::vector<int32_t> keep = s->task_rows;

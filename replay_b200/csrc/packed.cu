@@ -105,7 +105,7 @@ __device__ __forceinline__ int find_owner(const int32_t *off, int p) {
   return owner;
 }
 
-constexpr int kMaxTaskRows = 1024;  // rows of one task (host-side limit)
+constexpr int kMaxTaskRows = 4096;  // rows of one task (host-side limit)
 
 // Per-item hint byte (item = node x 4-word column): bit 0 an infection event
 // of this step (k_infect), bit 1 replicas that may move (E, I, waning R),
@@ -198,7 +198,21 @@ struct InfectQueue {
   int32_t nk;
 };
 
-constexpr int kInfectDynSmem = 2 * kEntBuf * 8 + 128 * 32 * 4 + kWarps * (int)sizeof(InfectQueue);
+// k_infect's dynamic shared memory, sized per launch: two staging buffers
+// and the warps' queues at fixed offsets, then the task's row pointers (max
+// task rows + 1), then a long row's per-replica exposures (int32,
+// min(32, q4) columns x 128 replicas).  Sized for the launch, so that tall
+// tasks or wide rows cost only where they occur (three CTAs per SM need at
+// most about 74 KB each).
+constexpr int kInfectQueueOff = 2 * kEntBuf * 8;
+constexpr int kInfectRpOff = kInfectQueueOff + kWarps * (int)sizeof(InfectQueue);
+__host__ __device__ constexpr int infect_acc_off(int max_rows) {
+  return (kInfectRpOff + 4 * (max_rows + 1) + 15) / 16 * 16;
+}
+__host__ __device__ constexpr int infect_smem(int q4, int max_rows) {
+  return infect_acc_off(max_rows) + (q4 < 32 ? q4 : 32) * 128 * 4;
+}
+constexpr int kInfectDynSmemMax = infect_smem(32, kMaxTaskRows);
 
 // Top 8 uniform bits of replica bit b from a queued word's planes.
 __device__ __forceinline__ uint32_t queued_top8(const uint4 (&q)[2], uint32_t b) {
@@ -443,7 +457,6 @@ __global__ void __launch_bounds__(kThreads, 3)
              const uint4 *__restrict__ sb, uint4 *__restrict__ evs,
              uint32_t *__restrict__ flag32, uint32_t step, float scale,
              const __grid_constant__ StepConsts c) {
-  __shared__ int32_t s_rp[kMaxTaskRows + 1];
   __shared__ float s_bw[128];  // max |beta_r| of each word of the slice
   __shared__ uint4 s_lor[32];  // long row: OR of the neighbours' masks per column
   __shared__ long long s_lemax;
@@ -451,10 +464,11 @@ __global__ void __launch_bounds__(kThreads, 3)
   extern __shared__ __align__(16) unsigned char s_dyn[];
   int2 *const s_buf0 = reinterpret_cast<int2 *>(s_dyn);  // two staging buffers of kEntBuf pairs
   auto bufp = [&](int b) { return s_buf0 + b * kEntBuf; };
+  InfectQueue &Q = reinterpret_cast<InfectQueue *>(s_dyn + kInfectQueueOff)[threadIdx.x >> 5];
+  // the task's row pointers (rows of a task <= L.max_task_rows)
+  int32_t *const s_rp = reinterpret_cast<int32_t *>(s_dyn + kInfectRpOff);
   // a long row's per-replica exposures (int32, ncols x 128 replicas)
-  int32_t *s_acc = reinterpret_cast<int32_t *>(s_dyn + 2 * kEntBuf * sizeof(int2));
-  InfectQueue &Q = reinterpret_cast<InfectQueue *>(
-      s_dyn + 2 * kEntBuf * sizeof(int2) + 128 * 32 * sizeof(float))[threadIdx.x >> 5];
+  int32_t *const s_acc = reinterpret_cast<int32_t *>(s_dyn + infect_acc_off(L.max_task_rows));
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t *mask_w = reinterpret_cast<const uint32_t *>(mask_in);
   uint32_t *evs_w = reinterpret_cast<uint32_t *>(evs);
@@ -744,7 +758,7 @@ __device__ __forceinline__ void count_bits(unsigned long long *s_ev, int wl, uin
 // Applies one word's moves; returns the new planes and counts the events.
 // Per-replica event counters of a task slice in shared memory, two 32-bit
 // words per replica (32-bit shared atomics): c0 = S->E | ->I << 16,
-// c1 = I-> | R->S << 16 (a task has at most 1024 rows).
+// c1 = I-> | R->S << 16 (a task has at most 4,096 rows).
 __device__ __forceinline__ void count_bits32(uint32_t *s_c, int wl, uint32_t t, uint32_t inc) {
   while (t) {
     const int r = __ffs(t) - 1;
@@ -1199,7 +1213,8 @@ rp_status packed_prepare() {
   cudaError_t e = cudaFuncSetAttribute(k_flow, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kFlowDynSmem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_flow)");
-  e = cudaFuncSetAttribute(k_infect, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfectDynSmem);
+  e = cudaFuncSetAttribute(k_infect, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kInfectDynSmemMax);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_infect)");
   return RP_OK;
 }
@@ -1234,7 +1249,7 @@ void packed_infect(const PackedLayout &L, const PackedTask *tasks, const int32_t
                    const int2 *entries, const uint32_t *mask, const uint32_t *sa,
                    const uint32_t *sb, uint32_t *evs, uint8_t *flag, uint32_t step, float scale,
                    const StepConsts &c, cudaStream_t st) {
-  k_infect<<<task_grid(L.n_tasks, 3), kThreads, kInfectDynSmem, st>>>(
+  k_infect<<<task_grid(L.n_tasks, 3), kThreads, infect_smem(L.q4, L.max_task_rows), st>>>(
       L, tasks, row_ptr, entries, reinterpret_cast<const uint4 *>(mask),
       reinterpret_cast<const uint4 *>(sa), reinterpret_cast<const uint4 *>(sb),
       reinterpret_cast<uint4 *>(evs), reinterpret_cast<uint32_t *>(flag), step, scale, c);

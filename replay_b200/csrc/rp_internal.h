@@ -329,6 +329,7 @@ struct PackedLayout {
   uint32_t last_mask; // valid bits of word vwords - 1
   int32_t lpr;        // lanes per row (power of 2, <= 32)
   int32_t n_tasks;
+  int32_t max_task_rows;  // rows of the tallest task
 };
 rp_status packed_prepare();  // kernel attributes, once per device
 void packed_init(const PackedLayout &L, uint32_t *sa, uint32_t *sb,
