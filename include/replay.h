@@ -301,15 +301,18 @@ RP_API rp_status rp_sim_profile_steps(rp_sim *s, float *step_ms);
 
 /* Tile autotuner of the batched path (no reference counterpart).  Networks
  * are bucketed by size (floor(log2 nodes)); for each bucket, largest first,
- * the task height (rows of one task: 32..4096) is chosen by timing the
- * replay's first `probe_steps` steps with CUDA events, keeping a candidate
- * only when it is 2% faster.  The simulation keeps the tuned tiles (and
- * re-captures its CUDA graph); results are unchanged by tiling.  Not for
- * simulations created with record_node_states. */
+ * the task height (rows of one task: 32..4096) and then the staging depth
+ * (CSR pairs the exposure kernel stages per chunk: 192, 384 or the default
+ * 768) are chosen by timing the replay's first `probe_steps` steps with
+ * CUDA events, keeping a candidate only when it is 2% faster.  The
+ * simulation keeps the tuned tiles (and re-captures its CUDA graph); results
+ * are unchanged by tiling.  Not for simulations created with
+ * record_node_states. */
 typedef struct {
   int32_t n_buckets;         /* network-size buckets */
   int32_t bucket_log2[32];   /* floor(log2 nodes) of each bucket */
   int32_t rows_per_task[32]; /* chosen task height, 0 = default kept */
+  int32_t stage_pairs[32];   /* chosen staging depth, 0 = default kept */
   int32_t probe_steps;       /* steps per timed probe */
   int32_t probes;            /* configurations timed */
   double ms_default;         /* probe time with the default tiles */

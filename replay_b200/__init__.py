@@ -248,14 +248,15 @@ class Simulation:
         return self._shape(counts)
 
     def autotune(self, probe_steps=48):
-        """Chooses the batched path's task height per network-size bucket by
-        timing the first probe_steps steps; returns the tuner's report."""
+        """Chooses the batched path's task height and staging depth per
+        network-size bucket by timing the first probe_steps steps; returns
+        the tuner's report (0 = default kept)."""
         r = _lib.TuneResult()
         check(lib().rp_sim_autotune(self._h, int(probe_steps), C.byref(r)))
         nb = r.n_buckets
         return {"buckets_log2": list(r.bucket_log2[:nb]), "rows_per_task": list(r.rows_per_task[:nb]),
-                "probe_steps": r.probe_steps, "probes": r.probes, "ms_default": r.ms_default,
-                "ms_tuned": r.ms_tuned}
+                "stage_pairs": list(r.stage_pairs[:nb]), "probe_steps": r.probe_steps, "probes": r.probes,
+                "ms_default": r.ms_default, "ms_tuned": r.ms_tuned}
 
     def run_text(self, write):
         """Runs the replay with node-state CSV lines formatted on the GPU;

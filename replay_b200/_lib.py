@@ -79,8 +79,8 @@ STATE_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_
 # Every entry point of include/replay.h with its ctypes signature.
 class TuneResult(C.Structure):
     _fields_ = [("n_buckets", C.c_int32), ("bucket_log2", C.c_int32 * 32), ("rows_per_task", C.c_int32 * 32),
-                ("probe_steps", C.c_int32), ("probes", C.c_int32), ("ms_default", C.c_double),
-                ("ms_tuned", C.c_double)]
+                ("stage_pairs", C.c_int32 * 32), ("probe_steps", C.c_int32), ("probes", C.c_int32),
+                ("ms_default", C.c_double), ("ms_tuned", C.c_double)]
 
 
 TEXT_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_char), C.c_size_t)

@@ -299,6 +299,7 @@ struct rp_sim {
   std::vector<int32_t> net_bounds;  // n_nets + 1 node offsets (empty: one network)
   std::vector<int32_t> h_first, h_rows;  // per network: first row, rows
   std::vector<int32_t> task_rows;        // per network: rows of one task
+  std::vector<int32_t> task_stage;       // per network: CSR pairs staged per chunk
   int32_t n_slices = 1;
   // node-state text mode (rp_sim_run_text)
   rp_text_cb text_cb = nullptr;
@@ -787,7 +788,7 @@ rp_status upload_tasks(rp_sim &s) {
     const int32_t f = s.h_first[net], e = f + s.h_rows[net];
     for (int32_t r0 = f; r0 < e; r0 += rpt)
       for (int32_t sl = 0; sl < s.n_slices; ++sl)
-        tasks.push_back(PackedTask{r0, std::min(r0 + rpt, e), sl, net * M});
+        tasks.push_back(PackedTask{r0, std::min(r0 + rpt, e), sl, net * M, s.task_stage[net]});
   }
   if (s.tasks.bytes < sizeof(PackedTask) * tasks.size())
     RP_TRY(s.tasks.alloc(sizeof(PackedTask) * tasks.size()));
@@ -845,6 +846,7 @@ rp_status alloc_state(rp_sim &s) {
   // default tiles: about 3 tasks per SM over the whole batch's rows (a
   // network smaller than a task is one task); rp_sim_autotune refines them
   s.task_rows.assign(s.n_nets, rows_per_task(N, n_slices));
+  s.task_stage.assign(s.n_nets, kStageDefault);
   RP_TRY(packed_prepare());
   RP_TRY(cd_prepare());
   const size_t plane = sizeof(uint32_t) * (size_t)N * L.words;
@@ -1564,7 +1566,8 @@ RP_API rp_status rp_sim_autotune(rp_sim *s, int32_t probe_steps, rp_tune_result 
   rp_status st = time_probe(best);
   const double ms_default = best;
   static const int32_t kCand[] = {32, 64, 128, 256, 512, 1024, 2048, 4096};
-  std::vector<int32_t> chosen(blist.size(), 0);
+  static const int32_t kStageCand[] = {192, 384};
+  std::vector<int32_t> chosen(blist.size(), 0), chosen_stage(blist.size(), 0);
   for (size_t bi = 0; bi < blist.size() && st == RP_OK; ++bi) {
     std::vector<int32_t> keep = s->task_rows;
     for (int32_t cand : kCand) {
@@ -1583,6 +1586,25 @@ RP_API rp_status rp_sim_autotune(rp_sim *s, int32_t probe_steps, rp_tune_result 
       s->task_rows = saved;
     }
     s->task_rows = keep;
+    // then the staging depth, with the bucket's chosen task height
+    std::vector<int32_t> keep_stage = s->task_stage;
+    for (int32_t cand : kStageCand) {
+      if (st != RP_OK) break;
+      std::vector<int32_t> saved = s->task_stage;
+      for (int k = 0; k < s->n_nets; ++k)
+        if (bucket[k] == blist[bi]) s->task_stage[k] = cand;
+      double ms = 0.0;
+      st = upload_tasks(*s);
+      if (st == RP_OK) st = time_probe(ms);
+      if (st != RP_OK) break;
+      if (ms < best * 0.98) {
+        best = ms;
+        keep_stage = s->task_stage;
+        chosen_stage[bi] = cand;
+      }
+      s->task_stage = saved;
+    }
+    s->task_stage = keep_stage;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1598,6 +1620,7 @@ RP_API rp_status rp_sim_autotune(rp_sim *s, int32_t probe_steps, rp_tune_result 
   for (size_t bi = 0; bi < blist.size(); ++bi) {
     out->bucket_log2[bi] = blist[bi];
     out->rows_per_task[bi] = chosen[bi];
+    out->stage_pairs[bi] = chosen_stage[bi];
   }
   out->probe_steps = probe;
   out->probes = probes;

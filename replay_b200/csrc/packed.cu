@@ -117,7 +117,7 @@ constexpr int kMaxTaskRows = 4096;  // rows of one task (host-side limit)
 // hints); elsewhere the extra work would not pay.
 constexpr uint8_t kFlagEvent = 1, kFlagActive = 2, kFlagSusceptible = 4;
 
-constexpr int kEntCap = 768;        // staged CSR pairs per chunk
+constexpr int kEntCap = kStageDefault;  // staging buffer capacity, CSR pairs
 constexpr int kEntBuf = kEntCap + 4; // a staging buffer (the copy may start one pair early)
 constexpr int kPiece = kEntBuf / 2 - 2;  // pairs per piece of a long row (a half buffer)
 constexpr long long kSpinLimit = 1ll << 22;
@@ -506,12 +506,14 @@ __global__ void __launch_bounds__(kThreads, 3)
         s_bw[wl] = mx;
       }
     __syncthreads();
-    // chunk of rows [r0, end) whose CSR pairs fit a staging buffer (>= 1 row)
+    // chunk of rows [r0, end) of at most `stage` CSR pairs (>= 1 row; the
+    // task's staging depth, at most a buffer)
+    const int32_t stage = T.stage < 1 || T.stage > kEntCap ? kEntCap : T.stage;
     auto chunk_end = [&](int r0) {
       int lo = r0 + 1, hi = nrows;
       while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (s_rp[mid] - s_rp[r0] <= kEntCap) lo = mid; else hi = mid - 1;
+        if (s_rp[mid] - s_rp[r0] <= stage) lo = mid; else hi = mid - 1;
       }
       return lo;
     };

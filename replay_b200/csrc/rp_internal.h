@@ -319,7 +319,9 @@ struct PackedTask {
   int32_t row_begin, row_end;  // rows of one network
   int32_t slice;               // 32 four-word columns (128 words) per slice
   int32_t count_base;          // index of replica 0 of this network in counts
+  int32_t stage;               // k_infect: CSR pairs staged per chunk (<= 768)
 };
+constexpr int32_t kStageDefault = 768;  // k_infect's staging buffer, in pairs
 struct PackedLayout {
   int32_t n_nodes;
   int32_t words;      // words per node row, padded to a multiple of 4

@@ -126,6 +126,7 @@ def test_autotune_keeps_results_and_reports():
     before = sim.run()
     rep = sim.autotune(probe_steps=10)
     assert sorted(rep["buckets_log2"], reverse=True) == rep["buckets_log2"] == [10, 9, 8, 6, 5]
-    assert rep["probes"] == 1 + 8 * 5 and rep["ms_tuned"] <= rep["ms_default"]
+    assert rep["probes"] == 1 + (8 + 2) * 5 and rep["ms_tuned"] <= rep["ms_default"]
     assert all(r in (0, 32, 64, 128, 256, 512, 1024, 2048, 4096) for r in rep["rows_per_task"])
+    assert all(r in (0, 192, 384) for r in rep["stage_pairs"])
     np.testing.assert_array_equal(sim.run(), before)
