@@ -460,6 +460,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ float s_bw[128];  // max |beta_r| of each word of the slice
   __shared__ uint4 s_lor[32];  // long row: OR of the neighbours' masks per column
   __shared__ long long s_lemax;
+  __shared__ int32_t s_stage;  // the task's staging depth (CSR pairs per chunk)
   __shared__ unsigned long long s_bar[4];  // chunk buffers 0, 1; long-row halves 0, 1
   extern __shared__ __align__(16) unsigned char s_dyn[];
   int2 *const s_buf0 = reinterpret_cast<int2 *>(s_dyn);  // two staging buffers of kEntBuf pairs
@@ -496,6 +497,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     const Div dv((uint32_t)ncols);
     const int nrows = T.row_end - T.row_begin;
     for (int i = threadIdx.x; i <= nrows; i += blockDim.x) s_rp[i] = row_ptr[T.row_begin + i];
+    if (threadIdx.x == 0) s_stage = T.stage < 1 || T.stage > kEntCap ? kEntCap : T.stage;
     if (c.beta_r)
       for (int wl = threadIdx.x; wl < ncols * 4; wl += blockDim.x) {
         float mx = 0.0f;
@@ -506,10 +508,11 @@ __global__ void __launch_bounds__(kThreads, 3)
         s_bw[wl] = mx;
       }
     __syncthreads();
-    // chunk of rows [r0, end) of at most `stage` CSR pairs (>= 1 row; the
-    // task's staging depth, at most a buffer)
-    const int32_t stage = T.stage < 1 || T.stage > kEntCap ? kEntCap : T.stage;
+    // chunk of rows [r0, end) of at most s_stage CSR pairs (>= 1 row; the
+    // task's staging depth, at most a buffer; read from shared memory so
+    // that it holds no register across the task)
     auto chunk_end = [&](int r0) {
+      const int32_t stage = s_stage;
       int lo = r0 + 1, hi = nrows;
       while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
