@@ -99,7 +99,7 @@ def _stratified(a, b, min_count=1500):
         z, p = _compare(a[:, ka == k], b[:, kb == k])
         zs.append(z[1:])  # t0 is the stratum itself
         ps.append(p)
-    return strata, np.concatenate(zs), ps
+    return strata, (np.concatenate(zs) if zs else np.zeros(0)), ps
 
 
 def test_matches_reference_cpu_path_in_distribution(runs):
@@ -146,8 +146,12 @@ def test_matches_reference_gpu_path_in_distribution(runs):
     inside, rms = _report(f"ours vs reference GPU path, {len(strata)} strata", z, min(ps))
     strata_c, zc, pc = _stratified(c, g)
     inside_c, rms_c = _report(f"reference CPU vs reference GPU path, {len(strata_c)} strata", zc, min(pc))
+    # each GPU run on its own (diagnostics only: a run holds a third of the
+    # pooled replicas, so its strata are smaller)
     for k in range(K):
-        _report(f"  GPU run {k}: ours", _stratified(a, ref_gpu[k])[1], 1.0)
-        _report(f"  GPU run {k}: reference CPU", _stratified(c, ref_gpu[k])[1], 1.0)
+        for name, x in (("ours", a), ("reference CPU", c)):
+            zk = _stratified(x, ref_gpu[k], min_count=1500 // K)[1]
+            if zk.size:
+                _report(f"  GPU run {k}: {name}", zk, 1.0)
     assert rms < 1.25 * rms_c + 2.5
     assert np.max(np.abs(z)) < 1.25 * np.max(np.abs(zc)) + 3.0
