@@ -653,13 +653,44 @@ __global__ void __launch_bounds__(kThreads, 3)
         __syncthreads();
       }
       const int nitems = skip_row || dense_done ? 0 : (r1 - r0) * ncols;
-      // warp-uniform; one pass past the items decides what is left queued
-      // (the staged pairs change with the next chunk)
-      for (int it0 = warp * 32;; it0 += kWarps * 32) {
-        const bool flushing = it0 >= nitems;
+      // warp-uniform passes; one pass past the items decides what is left
+      // queued (the staged pairs change with the next chunk)
+      int blk = warp * 32;  // this warp's next block of 32 items
+      // a chunk with fewer pairs than half its rows compacts its items
+      // (most of its rows have no pairs)
+      const bool sparse = 2 * (e1 - e0) < r1 - r0;
+      for (;;) {
+        // ---- phase 1a: in a sparse chunk, up to 32 items with CSR pairs
+        // from the warp's next blocks (many blocks fold into one pass; items
+        // without pairs have nothing to gather).  Their indices pass through
+        // Q.off, the rounds' scratch, which is free until the rounds ----
+        int got, it;
+        if (sparse) {
+          got = 0;
+          while (blk < nitems) {
+            const int itb = blk + lane;
+            bool has = false;
+            if (itb < nitems) {
+              const int rlb = (int)dv.div((uint32_t)itb);
+              has = s_rp[r0 + rlb + 1] > s_rp[r0 + rlb];
+            }
+            const unsigned hm = __ballot_sync(kFull, has);
+            if (got + __popc(hm) > 32) break;
+            if (has) Q.off[got + __popc(hm & ((1u << lane) - 1u))] = itb;
+            got += __popc(hm);
+            blk += kWarps * 32;
+          }
+          __syncwarp();
+          it = lane < got ? Q.off[lane] : 0;
+          __syncwarp();
+        } else {  // one block per pass
+          got = blk < nitems ? min(32, nitems - blk) : 0;
+          it = blk + lane;
+          blk += kWarps * 32;
+        }
+        const bool flushing = got == 0;
         // ---- phase 1: gather, per lane ----
-        const int it = it0 + lane;
-        const bool ok = it < nitems;
+        const bool ok = lane < got;
         const int rl = ok ? (int)dv.div((uint32_t)it) : 0;
         const int cc = ok ? it - rl * ncols : 0;
         const int rloc = r0 + rl;
