@@ -565,7 +565,7 @@ def meanfield_leg(replay_b200, g, net, p, nnz_total, hbm, reps=5):
     probability planes over all steps, per-node susceptibility ~ U[0.5, 1.5],
     adjoint checkpoints every 24 steps.  Times one forward and one backward
     (CUDA events, after warm-up), and calibrates beta against the Monte Carlo
-    daily incidence at a hidden beta = 3e-5, judged by the Monte Carlo."""
+    daily incidence at a hidden beta = 3e-5, checked against the Monte Carlo."""
     import torch
 
     from replay_b200.meanfield import MeanField, calibrate_beta, daily_incidence
@@ -606,7 +606,7 @@ def meanfield_leg(replay_b200, g, net, p, nnz_total, hbm, reps=5):
            "forward_ms": f, "backward_ms": b, "backward_over_forward": b / f,
            "forward_GBps": fwd_bytes / (f / 1e3) / 1e9, "forward_frac_of_hbm": fwd_bytes / (f / 1e3) / 1e9 / hbm}
 
-    # calibration: Monte Carlo target at a hidden beta, mean-field fit, Monte Carlo judge
+    # calibration: Monte Carlo target at a hidden beta, mean-field fit, Monte Carlo check
     mc = dict(p)
     mc.pop("beta_per_replica", None)
 
@@ -623,11 +623,11 @@ def meanfield_leg(replay_b200, g, net, p, nnz_total, hbm, reps=5):
     t0 = time.perf_counter()
     beta_cal, losses = calibrate_beta(mf, x0, target, beta0, susceptibility=sus, iters=40, lr=0.1, **rates)
     cal_s = time.perf_counter() - t0
-    judge = lambda b: float(((mc_daily(b, 202) - target) ** 2).mean())  # noqa: E731
+    mc_mse = lambda b: float(((mc_daily(b, 202) - target) ** 2).mean())  # noqa: E731
     out["calibration"] = {"beta_hidden": hidden, "beta_start": beta0, "beta_calibrated": beta_cal,
                           "iterations": len(losses), "seconds": cal_s, "mf_loss_first": losses[0],
-                          "mf_loss_last": losses[-1], "mc_judge_mse_calibrated": judge(beta_cal),
-                          "mc_judge_mse_start": judge(beta0)}
+                          "mf_loss_last": losses[-1], "mc_mse_calibrated": mc_mse(beta_cal),
+                          "mc_mse_start": mc_mse(beta0)}
     mf.close()
     return out
 

@@ -189,11 +189,11 @@ def test_calibrated_beta_reproduces_monte_carlo_incidence():
     print(f"beta_cal {beta_cal:.3e} loss {losses[0]:.3f} -> {losses[-1]:.3f}")
     assert losses[-1] < 0.2 * losses[0]
     assert beta_true / 2.5 < beta_cal < beta_true * 2.5
-    # the Monte Carlo judges: at the calibrated beta it reproduces the target
+    # the Monte Carlo checks the fit: at the calibrated beta it reproduces the target
     # curve far better than at the starting value
-    judge = lambda b: float(((_mc_daily(rb, g, p, b, 2, sus) - target) ** 2).mean())  # noqa: E731
-    j_cal, j0 = judge(beta_cal), judge(beta0)
-    print(f"MC judge: calibrated {j_cal:.3f} start {j0:.3f}")
+    mc_mse = lambda b: float(((_mc_daily(rb, g, p, b, 2, sus) - target) ** 2).mean())  # noqa: E731
+    j_cal, j0 = mc_mse(beta_cal), mc_mse(beta0)
+    print(f"MC mse: calibrated {j_cal:.3f} start {j0:.3f}")
     assert j_cal < 0.25 * j0
 
 
