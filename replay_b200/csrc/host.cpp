@@ -18,6 +18,7 @@
 #include <thread>
 #include <vector>
 
+#include "contact_prep.h"
 #include "rp_internal.h"
 
 namespace rp {
@@ -1082,19 +1083,13 @@ RP_API rp_status rp_graph_from_arrays(const int64_t *start, const int64_t *end,
   *out = nullptr;
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<int32_t> uu(n_contacts), vv(n_contacts);
-  std::vector<uint8_t> seen(n_nodes, 0);
   int32_t n_index = 0;
-  for (int64_t k = 0; k < n_contacts; ++k) {
-    if (u[k] < 0 || v[k] < 0 || u[k] >= n_nodes || v[k] >= n_nodes) {
-      set_error("contact %lld joins node outside [0, %d)", (long long)k, n_nodes);
-      return RP_ERR_ARG;
-    }
-    uu[k] = u[k] < v[k] ? u[k] : v[k];
-    vv[k] = u[k] < v[k] ? v[k] : u[k];
-    n_index += !seen[u[k]];
-    seen[u[k]] = 1;
-    n_index += !seen[v[k]];
-    seen[v[k]] = 1;
+  const int threads = (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+  const int64_t bad = prep_contacts(u, v, n_contacts, n_nodes, uu.data(), vv.data(), &n_index,
+                                    threads);
+  if (bad >= 0) {
+    set_error("contact %lld joins node outside [0, %d)", (long long)bad, n_nodes);
+    return RP_ERR_ARG;
   }
   std::unique_ptr<rp_graph> h(new rp_graph());
   h->g.device = device;
