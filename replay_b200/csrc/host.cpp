@@ -335,11 +335,7 @@ struct rp_sim {
     }
     if (text_len_host) cudaFreeHost(text_len_host);
     if (stream) cudaStreamDestroy(stream);
-    // work enqueued on a caller's stream may still read the buffers: the
-    // wait cudaFree would have made
-    if (g && cudaSetDevice(g->device) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess)
-      park.arm();
-    (void)cudaGetLastError();
+    if (g) park.arm_after_sync(g->device);
   }
 
   // Node-state CSV lines of one recorded step, formatted on the device in
@@ -587,8 +583,7 @@ struct rp_meanfield {
     if (fwd) cudaGraphExecDestroy(fwd);
     if (bwd) cudaGraphExecDestroy(bwd);
     if (cap) cudaStreamDestroy(cap);
-    if (cudaDeviceSynchronize() == cudaSuccess) park.arm();
-    (void)cudaGetLastError();
+    if (base.g) park.arm_after_sync(base.g->device);
   }
 };
 

@@ -61,6 +61,16 @@ struct ParkGuard {
       ++g_park;
     }
   }
+  // Waits for all work on `device` (the wait cudaFree would have made: work
+  // a caller enqueued on its own streams may still read the buffers), then
+  // arms; the caller's current device is left as it was.
+  void arm_after_sync(int device) {
+    int cur = 0;
+    const bool have_cur = cudaGetDevice(&cur) == cudaSuccess;
+    if (cudaSetDevice(device) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess) arm();
+    if (have_cur) cudaSetDevice(cur);
+    (void)cudaGetLastError();
+  }
   ~ParkGuard() {
     if (armed) --g_park;
   }
@@ -389,9 +399,5 @@ struct rp_graph {
   rp::ParkGuard park;  // destroyed after g: its blocks are kept for reuse
   rp::Graph g;
   double prep_ms = 0.0, build_ms = 0.0;  // creation phases (rp_graph_info)
-  ~rp_graph() {
-    if (cudaSetDevice(g.device) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess)
-      park.arm();
-    (void)cudaGetLastError();
-  }
+  ~rp_graph() { park.arm_after_sync(g.device); }
 };
