@@ -310,7 +310,10 @@ def run_ours(args, rank, world, local_rank):
         out["roofline"]["traffic_source"] = f"profiles/traffic.json: {capture}"
     out["profile_ms"] = {"per_step": prof} if args.no_extras else {"prebuilt": prof, "per_step": sim.profile()}
 
-    if not args.no_extras and rank == 0:
+    # the legs below are single-GPU measurements: a multi-GPU run (all GPUs
+    # held meanwhile) reports the step line only, and no rank waits in a
+    # collective the others do not enter
+    if not args.no_extras and world == 1:
         # ---- plain per-replica SpMV path (drop-in), same workload ----
         sim_plain = replay_b200.Simulation(g, path="plain", csr="prebuilt", **p)
         ms_plain = timed(sim_plain, 1, 1)
